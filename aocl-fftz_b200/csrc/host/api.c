@@ -1,0 +1,538 @@
+/* Public C ABI: aoclfftz_setup_* / execute / execute_io / destroy / version
+ * and the GPU extensions of aoclfftz_gpu.h (C99 host layer).
+ *
+ * Mirrors api/aoclfftz_api.c of the reference: setup validates the descriptor
+ * with the rules of api/validate_problem.h:346 and returns NULL on any failure;
+ * execute refuses NULL setup-time buffers (api/aoclfftz_api.c:66-82);
+ * execute_io lets the first concurrent caller use the plan's scratch and gives
+ * the others their own (api/aoclfftz_api.c:88-135) -- here a stream-ordered
+ * device allocation instead of a host slab.
+ */
+#include <cuda_runtime_api.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "aoclfftz_gpu.h"
+#include "fz_internal.h"
+
+static __thread char g_err[512];
+
+void fz_set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+static int g_log_mode = 0;
+
+void fz_log(const fz_plan *pl, const char *fmt, ...)
+{
+    int mode = pl ? pl->log_mode : g_log_mode;
+    if (mode < AOCLFFTZ_LOG_INFO) return;
+    va_list ap;
+    va_start(ap, fmt);
+    fprintf(stderr, "[aoclfftz-gpu] ");
+    vfprintf(stderr, fmt, ap);
+    fprintf(stderr, "\n");
+    va_end(ap);
+}
+
+const FFTZ_CHAR *aoclfftz_gpu_last_error(FFTZ_VOID) { return g_err; }
+
+/* ------------------------------------------------------------- validation */
+
+typedef struct
+{
+    void *in, *out;
+    int vec_rank, dim_rank;
+    fz_dim dims[16], vecs[16];
+    aoclfftz_flags_t *flags;
+    aoclfftz_cntrl_params_t *cp;
+    aoclfftz_smp_pfft_t *pt;
+} fz_desc;
+
+#define FZ_FAIL(...)                                                                                                   \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        fz_set_error(__VA_ARGS__);                                                                                     \
+        if (d->cp && d->cp->logger_mode >= AOCLFFTZ_LOG_INFO) fprintf(stderr, "[aoclfftz-gpu] %s\n", g_err);         \
+        return AOCLFFTZ_INVALID_INPUT;                                                                                 \
+    } while (0)
+
+/* the reference's VALIDATE_PROBLEM_DESCRIPTOR (api/validate_problem.h:346-414)
+ * and its helpers (:24-344), same checks in the same order */
+static int validate(fz_desc *d)
+{
+    aoclfftz_flags_t *f = d->flags;
+    aoclfftz_cntrl_params_t *cp = d->cp;
+    if (cp->logger_mode < 0 || cp->logger_mode > 3) cp->logger_mode = AOCLFFTZ_LOG_NONE;
+    if (cp->measure_stats != 0) cp->measure_stats = 0;
+    if (!cp->opt_off && (cp->opt_level < 0 || cp->opt_level > 3)) cp->opt_level = 3;
+    if (f->fft_type > 1) FZ_FAIL("fft_type can be Complex(0) or Real(1)");
+    if (f->fft_direction > 1) FZ_FAIL("fft_direction can be Forward(0) or Backward(1)");
+    if (f->storage_order) FZ_FAIL("out-of-order outputs are not supported");
+    if (f->fft_placement > 1) FZ_FAIL("fft_placement can be In-place(0) or Out-of-place(1)");
+    if (f->transpose_mode) FZ_FAIL("standalone transpose is not supported");
+    if (f->bit_reproducibility > 1) FZ_FAIL("bit_reproducibility can be Disable(0) or Enable(1)");
+    if (!f->fft_placement)
+    {
+        if (d->in != d->out) FZ_FAIL("input and output buffer must be the same for in-place problems");
+        if (!f->fft_type)
+        {
+            for (int i = 0; i < d->dim_rank; i++)
+                if (d->dims[i].is != d->dims[i].os) FZ_FAIL("dimension[%d]: in_stride != out_stride", i);
+            for (int i = 0; i < d->vec_rank; i++)
+                if (d->vecs[i].is != d->vecs[i].os) FZ_FAIL("vecs[%d]: in_stride != out_stride", i);
+        }
+        else
+        {
+            int64_t in_scale = f->fft_direction == 0 ? 2 : 1;
+            int64_t out_scale = f->fft_direction == 1 ? 2 : 1;
+            for (int i = 0; i < d->dim_rank; i++)
+                if (d->dims[i].is * out_scale != d->dims[i].os * in_scale)
+                {
+                    if (i == 0 && d->dims[i].is == d->dims[i].os) continue;
+                    FZ_FAIL("dimension[%d]: real in-place strides must differ by a factor of 2", i);
+                }
+            for (int i = 0; i < d->vec_rank; i++)
+                if (d->vecs[i].is * out_scale != d->vecs[i].os * in_scale && !(i == 0 && d->vecs[i].n == 1))
+                    FZ_FAIL("vecs[%d]: real in-place strides must differ by a factor of 2", i);
+        }
+    }
+    else if (d->in == d->out)
+        FZ_FAIL("input and output buffer cannot be the same for out-of-place problems");
+    if (d->pt->dynamic_load_model != 0 && d->pt->dynamic_load_model != 1) d->pt->dynamic_load_model = 1;
+    return AOCLFFTZ_SUCCESS;
+}
+
+/* ---------------------------------------------------------------- setup */
+
+static int64_t span_elems(const fz_dim *dims, int rank, const fz_dim *vecs, int vrank, int use_out, int64_t n0)
+{
+    int64_t s = 1;
+    for (int i = 0; i < rank; i++)
+    {
+        int64_t n = (i == 0 && n0 > 0) ? n0 : dims[i].n;
+        s += (n - 1) * (use_out ? dims[i].os : dims[i].is);
+    }
+    for (int i = 0; i < vrank; i++)
+        if (vecs[i].n > 0) s += (vecs[i].n - 1) * (use_out ? vecs[i].os : vecs[i].is);
+    return s;
+}
+
+static void plan_free(fz_plan *pl)
+{
+    if (!pl) return;
+    if (pl->dtab) cudaFree(pl->dtab);
+    if (pl->scratch) cudaFree(pl->scratch);
+    if (pl->stage) cudaFree(pl->stage);
+    free(pl->pass);
+    free(pl->blob.p);
+    pl->magic = 0;
+    free(pl);
+}
+
+static void *setup_impl(fz_desc *d, int dtype)
+{
+    fz_plan *pl = NULL;
+    g_err[0] = 0;
+    if (validate(d) != AOCLFFTZ_SUCCESS) return NULL;
+    g_log_mode = d->cp->logger_mode;
+    pl = (fz_plan *)calloc(1, sizeof(fz_plan));
+    if (!pl)
+    {
+        fz_set_error("out of host memory");
+        return NULL;
+    }
+    pl->magic = FZ_MAGIC;
+    pl->dtype = dtype;
+    pl->fft_type = d->flags->fft_type;
+    pl->direction = d->flags->fft_direction;
+    pl->placement = d->flags->fft_placement;
+    pl->log_mode = d->cp->logger_mode;
+    pl->setup_in = d->in;
+    pl->setup_out = d->out;
+    pl->stream = NULL;
+    if (cudaGetDevice(&pl->device) != cudaSuccess)
+    {
+        fz_set_error("no CUDA device available");
+        plan_free(pl);
+        return NULL;
+    }
+    const int64_t esz = dtype == 0 ? 4 : 8;
+    const int64_t n0 = d->dims[0].n;
+    if (pl->fft_type == 0)
+    {
+        pl->in_bytes = span_elems(d->dims, d->dim_rank, d->vecs, d->vec_rank, 0, 0) * 2 * esz;
+        pl->out_bytes = span_elems(d->dims, d->dim_rank, d->vecs, d->vec_rank, 1, 0) * 2 * esz;
+    }
+    else if (pl->direction == 0)
+    {
+        pl->in_bytes = span_elems(d->dims, d->dim_rank, d->vecs, d->vec_rank, 0, 0) * esz;
+        pl->out_bytes = span_elems(d->dims, d->dim_rank, d->vecs, d->vec_rank, 1, n0 / 2 + 1) * 2 * esz;
+    }
+    else
+    {
+        pl->in_bytes = span_elems(d->dims, d->dim_rank, d->vecs, d->vec_rank, 0, n0 / 2 + 1) * 2 * esz;
+        pl->out_bytes = span_elems(d->dims, d->dim_rank, d->vecs, d->vec_rank, 1, 0) * esz;
+    }
+    if (fz_plan_build(pl, d->dim_rank, d->dims, d->vec_rank, d->vecs))
+    {
+        fz_log(pl, "setup failed: %s", g_err);
+        plan_free(pl);
+        return NULL;
+    }
+    /* device tables: one allocation, then every pass's pointers */
+    if (pl->blob.len)
+    {
+        if (cudaMalloc(&pl->dtab, pl->blob.len) != cudaSuccess ||
+            cudaMemcpy(pl->dtab, pl->blob.p, pl->blob.len, cudaMemcpyHostToDevice) != cudaSuccess)
+        {
+            cudaGetLastError();
+            fz_set_error("device allocation of %zu table bytes failed", pl->blob.len);
+            plan_free(pl);
+            return NULL;
+        }
+    }
+    for (int i = 0; i < pl->npass; i++)
+    {
+        fz_pass *p = &pl->pass[i];
+        unsigned char *base = (unsigned char *)pl->dtab;
+        p->k.tw = p->off_tw >= 0 ? base + p->off_tw : NULL;
+        p->k.tw4_hi = p->off_tw4hi >= 0 ? base + p->off_tw4hi : NULL;
+        p->k.tw4_lo = p->off_tw4lo >= 0 ? base + p->off_tw4lo : NULL;
+        p->k.pre_tab = p->off_pre >= 0 ? base + p->off_pre : NULL;
+        p->k.post_tab = p->off_post >= 0 ? base + p->off_post : NULL;
+        p->k.mid_tab = p->off_mid >= 0 ? base + p->off_mid : NULL;
+        p->k.rtw = p->off_rtw >= 0 ? base + p->off_rtw : NULL;
+    }
+    pl->nlaunch = pl->npass;
+    const int64_t csz = 2 * esz;
+    int64_t s0 = pl->scratch_elems[0] * csz, s1 = pl->scratch_elems[1] * csz;
+    s0 = (s0 + 255) & ~(int64_t)255;
+    pl->scratch_bytes = s0 + s1;
+    if (pl->scratch_bytes > 0 && cudaMalloc(&pl->scratch, (size_t)pl->scratch_bytes) != cudaSuccess)
+    {
+        cudaGetLastError();
+        fz_set_error("device allocation of %lld scratch bytes failed", (long long)pl->scratch_bytes);
+        plan_free(pl);
+        return NULL;
+    }
+    if (pl->log_mode >= AOCLFFTZ_LOG_INFO)
+    {
+        char buf[1024];
+        aoclfftz_gpu_describe(pl, buf, sizeof(buf));
+        fz_log(pl, "plan: %s", buf);
+    }
+    return pl;
+}
+
+#define FILL_DESC(problem)                                                                                             \
+    fz_desc d;                                                                                                         \
+    memset(&d, 0, sizeof(d));                                                                                          \
+    if (!(problem))                                                                                                    \
+    {                                                                                                                  \
+        fz_set_error("problem descriptor is NULL");                                                                    \
+        return NULL;                                                                                                   \
+    }                                                                                                                  \
+    d.in = (problem)->in;                                                                                              \
+    d.out = (problem)->out;                                                                                            \
+    d.vec_rank = (problem)->vec_rank;                                                                                  \
+    d.dim_rank = (problem)->dim_rank;                                                                                  \
+    d.flags = &(problem)->flags;                                                                                       \
+    d.cp = &(problem)->cntrl_params;                                                                                   \
+    d.pt = &(problem)->pthr_fft;                                                                                       \
+    if (d.dim_rank <= 0)                                                                                               \
+    {                                                                                                                  \
+        fz_set_error("dim rank must be at least 1");                                                                   \
+        return NULL;                                                                                                   \
+    }                                                                                                                  \
+    if (d.vec_rank <= 0)                                                                                               \
+    {                                                                                                                  \
+        fz_set_error("vec rank must be at least 1");                                                                   \
+        return NULL;                                                                                                   \
+    }                                                                                                                  \
+    if (d.dim_rank > 16 || d.vec_rank > 16)                                                                            \
+    {                                                                                                                  \
+        fz_set_error("ranks above 16 are not supported");                                                             \
+        return NULL;                                                                                                   \
+    }                                                                                                                  \
+    if (!(problem)->dims)                                                                                              \
+    {                                                                                                                  \
+        fz_set_error("dims cannot be NULL");                                                                           \
+        return NULL;                                                                                                   \
+    }                                                                                                                  \
+    for (int i_ = 0; i_ < d.dim_rank; i_++)                                                                            \
+    {                                                                                                                  \
+        d.dims[i_].n = (problem)->dims[i_].n;                                                                          \
+        d.dims[i_].is = (problem)->dims[i_].in_stride;                                                                 \
+        d.dims[i_].os = (problem)->dims[i_].out_stride;                                                                \
+        if (d.dims[i_].n <= 0 || d.dims[i_].is <= 0 || d.dims[i_].os <= 0)                                             \
+        {                                                                                                              \
+            fz_set_error("dimension[%d]: size and strides must be positive", i_);                                     \
+            return NULL;                                                                                               \
+        }                                                                                                              \
+    }                                                                                                                  \
+    if (!(problem)->vecs)                                                                                              \
+    {                                                                                                                  \
+        fz_set_error("vecs cannot be NULL");                                                                           \
+        return NULL;                                                                                                   \
+    }                                                                                                                  \
+    for (int i_ = 0; i_ < d.vec_rank; i_++)                                                                            \
+    {                                                                                                                  \
+        d.vecs[i_].n = (problem)->vecs[i_].n;                                                                          \
+        d.vecs[i_].is = (problem)->vecs[i_].in_stride;                                                                 \
+        d.vecs[i_].os = (problem)->vecs[i_].out_stride;                                                                \
+        if (d.vecs[i_].n < 0 || d.vecs[i_].is <= 0 || d.vecs[i_].os <= 0)                                              \
+        {                                                                                                              \
+            fz_set_error("vector[%d]: size must be >= 0 and strides positive", i_);                                   \
+            return NULL;                                                                                               \
+        }                                                                                                              \
+    }
+
+FFTZ_VOID *aoclfftz_setup_f(aoclfftz_prob_desc_f *problem)
+{
+    FILL_DESC(problem)
+    return setup_impl(&d, 0);
+}
+
+FFTZ_VOID *aoclfftz_setup_d(aoclfftz_prob_desc_d *problem)
+{
+    FILL_DESC(problem)
+    return setup_impl(&d, 1);
+}
+
+FFTZ_VOID *aoclfftz_setup_f_64_(aoclfftz_prob_desc_f_64_ *problem)
+{
+    FILL_DESC(problem)
+    return setup_impl(&d, 0);
+}
+
+FFTZ_VOID *aoclfftz_setup_d_64_(aoclfftz_prob_desc_d_64_ *problem)
+{
+    FILL_DESC(problem)
+    return setup_impl(&d, 1);
+}
+
+/* -------------------------------------------------------------- execute */
+
+static fz_plan *as_plan(void *h)
+{
+    fz_plan *pl = (fz_plan *)h;
+    if (!pl || pl->magic != FZ_MAGIC) return NULL;
+    return pl;
+}
+
+/* 1 if the GPU can use the pointer directly (device or managed memory) */
+static int device_usable(const void *p)
+{
+    struct cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static aoclfftz_error_type run(fz_plan *pl, void *in, void *out)
+{
+    if (pl->nop) return AOCLFFTZ_SUCCESS;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != pl->device) cudaSetDevice(pl->device);
+    cudaStream_t st = (cudaStream_t)pl->stream;
+    const int in_dev = device_usable(in);
+    const int out_dev = device_usable(out);
+    const int inplace = (in == out);
+    /* ownership of the plan's scratch and staging memory */
+    int expected = 0;
+    const int owner = __atomic_compare_exchange_n(&pl->scratch_busy, &expected, 1, 0, __ATOMIC_ACQ_REL,
+                                                  __ATOMIC_ACQUIRE);
+    void *scratch = NULL, *stage = NULL;
+    int64_t stage_need = 0;
+    if (!in_dev || !out_dev)
+    {
+        int64_t a = (pl->in_bytes + 255) & ~(int64_t)255;
+        stage_need = inplace ? (pl->in_bytes > pl->out_bytes ? pl->in_bytes : pl->out_bytes) : a + pl->out_bytes;
+    }
+    aoclfftz_error_type ret = AOCLFFTZ_SUCCESS;
+    if (owner)
+    {
+        scratch = pl->scratch;
+        if (stage_need > pl->stage_bytes)
+        {
+            if (pl->stage) cudaFree(pl->stage);
+            pl->stage = NULL;
+            pl->stage_bytes = 0;
+            if (cudaMalloc(&pl->stage, (size_t)stage_need) != cudaSuccess)
+            {
+                cudaGetLastError();
+                fz_set_error("staging allocation of %lld bytes failed", (long long)stage_need);
+                __atomic_store_n(&pl->scratch_busy, 0, __ATOMIC_RELEASE);
+                return AOCLFFTZ_MEMORY_FAILURE;
+            }
+            pl->stage_bytes = stage_need;
+        }
+        stage = pl->stage;
+    }
+    else
+    {
+        if (pl->scratch_bytes > 0 && cudaMallocAsync(&scratch, (size_t)pl->scratch_bytes, st) != cudaSuccess)
+        {
+            cudaGetLastError();
+            fz_set_error("per-call scratch allocation failed");
+            return AOCLFFTZ_MEMORY_FAILURE;
+        }
+        if (stage_need > 0 && cudaMallocAsync(&stage, (size_t)stage_need, st) != cudaSuccess)
+        {
+            cudaGetLastError();
+            if (scratch) cudaFreeAsync(scratch, st);
+            fz_set_error("per-call staging allocation failed");
+            return AOCLFFTZ_MEMORY_FAILURE;
+        }
+    }
+    void *buf[FZ_NBUF];
+    buf[FZ_BUF_IN] = in;
+    buf[FZ_BUF_OUT] = out;
+    if (!in_dev || !out_dev)
+    {
+        unsigned char *sb = (unsigned char *)stage;
+        void *din = in_dev ? in : (void *)sb;
+        void *dout = out_dev ? out : (inplace ? (void *)sb : (void *)(sb + ((pl->in_bytes + 255) & ~(int64_t)255)));
+        if (!in_dev && cudaMemcpyAsync(din, in, (size_t)pl->in_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            ret = AOCLFFTZ_EXECUTION_FAILURE;
+        buf[FZ_BUF_IN] = din;
+        buf[FZ_BUF_OUT] = dout;
+    }
+    int64_t s0 = (pl->scratch_elems[0] * 2 * (pl->dtype == 0 ? 4 : 8) + 255) & ~(int64_t)255;
+    buf[FZ_BUF_S0] = scratch;
+    buf[FZ_BUF_S1] = scratch ? (void *)((unsigned char *)scratch + s0) : NULL;
+    for (int i = 0; i < pl->npass && ret == AOCLFFTZ_SUCCESS; i++)
+    {
+        fftz_pass_t k = pl->pass[i].k;
+        k.in = buf[pl->pass[i].src];
+        k.out = buf[pl->pass[i].dst];
+        int e = fftz_launch_pass(&k, st);
+        if (e != 0)
+        {
+            fz_set_error("launch of pass %d (%s) failed: %s", i, pl->pass[i].what, cudaGetErrorString((cudaError_t)e));
+            ret = AOCLFFTZ_EXECUTION_FAILURE;
+        }
+    }
+    if (ret == AOCLFFTZ_SUCCESS && !out_dev)
+    {
+        if (cudaMemcpyAsync(out, buf[FZ_BUF_OUT], (size_t)pl->out_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            ret = AOCLFFTZ_EXECUTION_FAILURE;
+    }
+    if (!owner)
+    {
+        if (scratch) cudaFreeAsync(scratch, st);
+        if (stage) cudaFreeAsync(stage, st);
+    }
+    if (!in_dev || !out_dev || !owner)
+    {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+        {
+            fz_set_error("execution failed: %s", cudaGetErrorString(e));
+            ret = AOCLFFTZ_EXECUTION_FAILURE;
+        }
+    }
+    if (owner) __atomic_store_n(&pl->scratch_busy, 0, __ATOMIC_RELEASE);
+    return ret;
+}
+
+aoclfftz_error_type aoclfftz_execute(FFTZ_VOID *handle)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl) return AOCLFFTZ_EXECUTION_FAILURE;
+    if (!pl->setup_in || !pl->setup_out)
+    {
+        fz_set_error("one or both setup-time buffers are NULL; use aoclfftz_execute_io");
+        return AOCLFFTZ_EXECUTION_FAILURE;
+    }
+    return run(pl, pl->setup_in, pl->setup_out);
+}
+
+aoclfftz_error_type aoclfftz_execute_io(FFTZ_VOID *handle, FFTZ_VOID *in, FFTZ_VOID *out)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl || !in || !out) return AOCLFFTZ_EXECUTION_FAILURE;
+    if ((pl->placement == 0) != (in == out))
+    {
+        fz_set_error("buffers do not match the plan's placement");
+        return AOCLFFTZ_EXECUTION_FAILURE;
+    }
+    return run(pl, in, out);
+}
+
+FFTZ_VOID aoclfftz_destroy(FFTZ_VOID *handle)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl) return;
+    if (pl->stream) cudaStreamSynchronize((cudaStream_t)pl->stream);
+    else cudaDeviceSynchronize();
+    plan_free(pl);
+}
+
+const FFTZ_CHAR *aoclfftz_version(FFTZ_VOID) { return AOCLFFTZ_LIBRARY_VERSION " B200 (sm_100a)"; }
+
+/* ------------------------------------------------------- GPU extensions */
+
+aoclfftz_error_type aoclfftz_gpu_set_stream(FFTZ_VOID *handle, FFTZ_VOID *stream)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl) return AOCLFFTZ_INVALID_INPUT;
+    pl->stream = stream;
+    return AOCLFFTZ_SUCCESS;
+}
+
+FFTZ_VOID *aoclfftz_gpu_get_stream(FFTZ_VOID *handle)
+{
+    fz_plan *pl = as_plan(handle);
+    return pl ? pl->stream : NULL;
+}
+
+aoclfftz_error_type aoclfftz_gpu_synchronize(FFTZ_VOID *handle)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl) return AOCLFFTZ_INVALID_INPUT;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)pl->stream);
+    if (e != cudaSuccess)
+    {
+        fz_set_error("%s", cudaGetErrorString(e));
+        return AOCLFFTZ_EXECUTION_FAILURE;
+    }
+    return AOCLFFTZ_SUCCESS;
+}
+
+FFTZ_INT32 aoclfftz_gpu_num_launches(FFTZ_VOID *handle)
+{
+    fz_plan *pl = as_plan(handle);
+    return pl ? (pl->nop ? 0 : pl->nlaunch) : -1;
+}
+
+FFTZ_INT32 aoclfftz_gpu_describe(FFTZ_VOID *handle, FFTZ_CHAR *buf, FFTZ_INT32 len)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl || !buf || len <= 0) return -1;
+    int w = snprintf(buf, (size_t)len, "%s %s %s %s:", pl->dtype ? "f64" : "f32", pl->fft_type ? "real" : "c2c",
+                     pl->direction ? "bwd" : "fwd", pl->placement ? "oop" : "inplace");
+    if (pl->nop && w < len) w += snprintf(buf + w, (size_t)(len - w), " empty batch");
+    for (int i = 0; i < pl->npass && w < len; i++)
+        w += snprintf(buf + w, (size_t)(len - w), " [%s tpc=%d tpt=%d]", pl->pass[i].what, pl->pass[i].k.tpc,
+                      pl->pass[i].k.tpt);
+    return w < len ? w : len - 1;
+}
+
+FFTZ_INT64 aoclfftz_gpu_device_bytes(FFTZ_VOID *handle)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl) return -1;
+    return (FFTZ_INT64)pl->blob.len + pl->scratch_bytes + pl->stage_bytes;
+}

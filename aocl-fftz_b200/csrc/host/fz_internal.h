@@ -1,0 +1,93 @@
+/* Internal plan structures of the B200 FFT library (C99 host layer).
+ *
+ * A plan is a flat list of kernel passes (fftz_pass_t, see
+ * ../kernels/fftz_kernels.h) over four logical buffers: the caller's input,
+ * the caller's output and two plan-owned scratch arrays. The reference keeps a
+ * linked tree of solver nodes walked at execute time
+ * (api/aoclfftz_internal.h:797-805, core/executor.c:17-44); on the GPU the
+ * tree is flattened at setup into this pass list, so execute is a loop of
+ * kernel launches with no host-side recursion.
+ */
+#ifndef FZ_INTERNAL_H
+#define FZ_INTERNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../kernels/fftz_kernels.h"
+#include "aoclfftz.h"
+
+#define FZ_MAGIC 0x475a4646u /* "FFZG" */
+
+enum { FZ_BUF_IN = 0, FZ_BUF_OUT = 1, FZ_BUF_S0 = 2, FZ_BUF_S1 = 3, FZ_NBUF = 4 };
+
+/* one tensor dimension, strides in elements of the side's type */
+typedef struct
+{
+    int64_t n, is, os;
+} fz_dim;
+
+typedef struct
+{
+    fftz_pass_t k;
+    int src, dst;
+    /* byte offsets of the pass's tables in the plan's table blob (-1: none) */
+    int64_t off_tw, off_tw4hi, off_tw4lo, off_pre, off_post, off_mid, off_rtw;
+    char what[64];
+} fz_pass;
+
+/* growable host byte buffer holding every table of a plan before upload */
+typedef struct
+{
+    unsigned char *p;
+    size_t len, cap;
+} fz_blob;
+
+typedef struct fz_plan
+{
+    uint32_t magic;
+    int dtype;     /* 0 float, 1 double */
+    int fft_type;  /* 0 complex, 1 real */
+    int direction; /* 0 forward, 1 backward */
+    int placement; /* 0 in-place, 1 out-of-place */
+    int log_mode;
+    int nop;       /* empty batch: execute succeeds without work */
+    void *setup_in, *setup_out;
+    int64_t in_bytes, out_bytes; /* bytes spanned by the input / output buffers */
+    int npass, cap;
+    fz_pass *pass;
+    fz_blob blob;
+    int64_t scratch_elems[2]; /* complex elements of S0, S1 */
+    /* device state */
+    int device;
+    void *dtab;
+    void *scratch; /* S0 then S1 in one allocation */
+    int64_t scratch_bytes;
+    void *stage; /* staging buffer for host-memory callers (in, then out) */
+    int64_t stage_bytes;
+    void *stream; /* cudaStream_t; NULL = legacy default stream */
+    int scratch_busy; /* 1 while an execute holds the plan's scratch */
+    int nlaunch;
+} fz_plan;
+
+/* ---- logging / errors (api.c) ---- */
+void fz_set_error(const char *fmt, ...);
+void fz_log(const fz_plan *pl, const char *fmt, ...);
+
+/* ---- tables (tables.c) ---- */
+int64_t fz_blob_add(fz_blob *b, const void *data, size_t bytes);
+int64_t fz_blob_reserve(fz_blob *b, size_t bytes);
+/* stage twiddles for a radix list; returns blob offset, fills tw_off[] */
+int64_t fz_stage_twiddles(fz_blob *b, int dtype, int n, int nstages, const int32_t *radix, int32_t *tw_off);
+/* four-step factor tables W_N^(hi*L), W_N^lo as double2 */
+int fz_tw4_tables(fz_blob *b, int64_t N, int64_t *L, int64_t *off_hi, int64_t *off_lo);
+/* Bluestein tables for length n, pow2 convolution length m, direction */
+int fz_bluestein_tables(fz_blob *b, int dtype, int64_t n, int64_t m, int direction, int64_t *off_pre,
+                        int64_t *off_post, int64_t *off_mid);
+/* packed-real twiddles W_{2M}^k, k = 0..M (W^M = -1) */
+int64_t fz_real_twiddles(fz_blob *b, int dtype, int64_t M);
+
+/* ---- planner (plan.c) ---- */
+int fz_plan_build(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const fz_dim *vecs);
+
+#endif

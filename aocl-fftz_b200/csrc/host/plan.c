@@ -1,0 +1,711 @@
+/* Planner: problem descriptor -> flat list of GPU kernel passes (C99).
+ *
+ * The reference's selector walks a rule tree (selector/selector.c:509-789):
+ * pow2 iterative for in-cache powers of two, four-step beyond the cache
+ * (:603-633), batched / N-D row-column (:660-694), Bluestein when no kernel
+ * radix divides N (:701-717), Cooley-Tukey otherwise (:772-786), and the
+ * packed real path for even real lengths (:858-874). The same decisions are
+ * made here against the GPU's limits instead of the CPU's caches:
+ *
+ *   line of length n fits one CTA's shared memory
+ *       -> one pass (compile-time kernel for powers of two, generic otherwise)
+ *   n too long for one CTA, all factors in {2,3,5,7,11,13}
+ *       -> four-step n = n1 * n2 in two passes through scratch
+ *          (column FFTs with the W_n^{j2 k1} twiddle fused into their store,
+ *           then row FFTs whose store performs the transpose)
+ *   any prime factor > 13
+ *       -> Bluestein over a power-of-two convolution length m >= 2n - 1, in one
+ *          kernel when m fits shared memory, in four passes otherwise
+ *   N-D -> one line pass per dimension (dims[0] first, the rest in place)
+ *   real, dims[0] even -> packed: n0/2-point complex FFT with the Hermitian
+ *          recombination fused into the store (r2c) or the separation fused
+ *          into the load (c2r); odd n0 -> full-length complex line.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "fz_internal.h"
+
+static int is_pow2(int64_t n) { return n > 0 && (n & (n - 1)) == 0; }
+
+static int ilog2i(int64_t n)
+{
+    int k = 0;
+    while (((int64_t)1 << k) < n) k++;
+    return k;
+}
+
+static int smooth13(int64_t n)
+{
+    static const int64_t pr[] = {2, 3, 5, 7, 11, 13};
+    for (int i = 0; i < 6; i++)
+        while (n % pr[i] == 0) n /= pr[i];
+    return n == 1;
+}
+
+/* radix list of the generic kernel: balanced power-of-two part (<= 16 per
+ * stage, largest first) followed by the odd prime factors */
+static int generic_radices(int64_t n, int32_t *radix)
+{
+    int s = 0;
+    int k = 0;
+    while ((n & 1) == 0)
+    {
+        n >>= 1;
+        k++;
+    }
+    if (k > 0)
+    {
+        int st = (k + 3) / 4;
+        int base = k / st, extra = k % st;
+        for (int i = 0; i < st; i++)
+        {
+            if (s >= FFTZ_MAX_STAGES) return -1;
+            radix[s++] = 1 << (base + (i < extra ? 1 : 0));
+        }
+    }
+    static const int64_t odd[] = {13, 11, 7, 5, 3};
+    for (int i = 0; i < 5; i++)
+        while (n % odd[i] == 0)
+        {
+            if (s >= FFTZ_MAX_STAGES) return -1;
+            radix[s++] = (int32_t)odd[i];
+            n /= odd[i];
+        }
+    return n == 1 ? s : -1;
+}
+
+static fz_pass *push_pass(fz_plan *pl)
+{
+    if (pl->npass == pl->cap)
+    {
+        int nc = pl->cap ? pl->cap * 2 : 8;
+        fz_pass *np = (fz_pass *)realloc(pl->pass, sizeof(fz_pass) * (size_t)nc);
+        if (!np) return NULL;
+        pl->pass = np;
+        pl->cap = nc;
+    }
+    fz_pass *p = &pl->pass[pl->npass++];
+    memset(p, 0, sizeof(*p));
+    p->off_tw = p->off_tw4hi = p->off_tw4lo = p->off_pre = p->off_post = p->off_mid = p->off_rtw = -1;
+    p->k.dtype = pl->dtype;
+    p->k.scale = 1.0;
+    return p;
+}
+
+static int64_t absl(int64_t x) { return x < 0 ? -x : x; }
+
+/* Batch dims: optionally sorted by stride (smallest first, so that bdim[0]
+ * is the one lanes may run along), then adjacent dims merged when they form
+ * one arithmetic progression on both sides (the reference's fuse_vecs,
+ * selector/selector.c:1861-1912). keep_first pins b[0] as the column dim. */
+static int set_batch(fftz_pass_t *k, const fz_dim *b, int nb, int keep_first)
+{
+    fz_dim d[32];
+    int m = 0;
+    for (int i = 0; i < nb && m < 32; i++)
+        if (b[i].n != 1) d[m++] = b[i];
+    if (m == 0 && keep_first && nb > 0) d[m++] = b[0];
+    int start = keep_first ? 1 : 0;
+    for (int i = start + 1; i < m; i++)
+        for (int j = i; j > start; j--)
+        {
+            int64_t sj = absl(d[j].is) < absl(d[j].os) ? absl(d[j].is) : absl(d[j].os);
+            int64_t sp = absl(d[j - 1].is) < absl(d[j - 1].os) ? absl(d[j - 1].is) : absl(d[j - 1].os);
+            if (sj < sp)
+            {
+                fz_dim t = d[j];
+                d[j] = d[j - 1];
+                d[j - 1] = t;
+            }
+        }
+    /* merge neighbours that continue one another on both sides; a pinned
+     * column dim stays separate because its index is the column number */
+    int w = 0;
+    for (int i = 0; i < m; i++)
+    {
+        if (w > 0 && !(keep_first && w == 1) && d[i].is == d[w - 1].is * d[w - 1].n &&
+            d[i].os == d[w - 1].os * d[w - 1].n)
+        {
+            d[w - 1].n *= d[i].n;
+            continue;
+        }
+        d[w++] = d[i];
+    }
+    if (w > FFTZ_MAX_BDIMS)
+    {
+        fz_set_error("too many independent batch dimensions (%d > %d)", w, FFTZ_MAX_BDIMS);
+        return -1;
+    }
+    k->nbdims = w;
+    k->ntf = 1;
+    for (int i = 0; i < w; i++)
+    {
+        k->bdim[i] = d[i].n;
+        k->ibs[i] = d[i].is;
+        k->obs[i] = d[i].os;
+        k->ntf *= d[i].n;
+    }
+    return 0;
+}
+
+/* transforms per CTA: enough columns for coalesced column access, enough
+ * work per CTA for short rows, bounded by threads and shared memory */
+static void finish_launch_shape(fz_plan *pl, fftz_pass_t *k, int nslots, int maxthr)
+{
+    const int64_t esz = pl->dtype == 0 ? 8 : 16;
+    k->sstride = fftz_smem_stride(pl->dtype, nslots);
+    int by_thr = maxthr / k->tpt;
+    if (by_thr < 1) by_thr = 1;
+    int64_t by_smem = fftz_smem_limit() / ((int64_t)k->sstride * esz + 24);
+    int want;
+    if (k->in_mode == 1 || k->out_mode == 1)
+        want = pl->dtype == 0 ? 8 : 4; /* 64-byte column segments */
+    else
+    {
+        int64_t per = pl->dtype == 0 ? 4096 : 2048; /* complex elements per CTA */
+        want = (int)((per + k->n - 1) / k->n);
+        if (want * k->tpt < 128) want = (128 + k->tpt - 1) / k->tpt;
+    }
+    int tpc = want;
+    if (tpc > by_thr) tpc = by_thr;
+    if (tpc > by_smem) tpc = (int)by_smem;
+    if (tpc > k->ntf) tpc = (int)k->ntf;
+    if (tpc > 1024) tpc = 1024;
+    if (tpc < 1) tpc = 1;
+    k->tpc = tpc;
+}
+
+static void set_modes(fftz_pass_t *k)
+{
+    k->in_mode = (k->nbdims > 0 && absl(k->ibs[0]) < absl(k->ies)) ? 1 : 0;
+    k->out_mode = (k->nbdims > 0 && absl(k->obs[0]) < absl(k->oes)) ? 1 : 0;
+}
+
+/* one complex line pass in the shared-memory kernel; returns the pass */
+static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_dim *b, int nb,
+                          int keep_first, int src, int dst, int flags, int variant_bits)
+{
+    fz_pass *p = push_pass(pl);
+    if (!p) return NULL;
+    fftz_pass_t *k = &p->k;
+    k->n = (int32_t)n;
+    k->ies = ies;
+    k->oes = oes;
+    k->flags = flags;
+    k->in_kind = FFTZ_IN_COMPLEX;
+    k->out_kind = FFTZ_OUT_COMPLEX;
+    k->nload = (int32_t)n;
+    k->nstore = (int32_t)n;
+    p->src = src;
+    p->dst = dst;
+    if (set_batch(k, b, nb, keep_first)) return NULL;
+    set_modes(k);
+    const int fast = is_pow2(n) && n >= 2 && n <= fftz_fast_max_n(pl->dtype);
+    int maxthr;
+    if (fast)
+    {
+        k->nstages = fftz_fast_radices((int)n, k->radix);
+        k->tpt = fftz_fast_tpt((int)n);
+        maxthr = pl->dtype == 0 ? 1024 : 512;
+        if (k->nstages == 1 && k->in_mode != k->out_mode) k->out_mode = k->in_mode;
+        int tabs = (variant_bits & 2) != 0, tw4 = (flags & FFTZ_F_TW4) != 0;
+        if (variant_bits & 4)
+            k->variant = FFTZ_VAR_FAST_BLUE;
+        else if (tabs && tw4)
+            k->variant = FFTZ_VAR_FAST_TW4_TABS;
+        else if (tabs)
+            k->variant = FFTZ_VAR_FAST_TABS;
+        else if (tw4)
+            k->variant = FFTZ_VAR_FAST_TW4;
+        else
+            k->variant = FFTZ_VAR_FAST;
+        if ((tw4 || tabs) && n < 32 && !(variant_bits & 4))
+        {
+            /* small feature kernels are not instantiated: use the generic one */
+            goto generic;
+        }
+        k->fuse_load = 1;
+        k->fuse_store = 1;
+    }
+    else
+    {
+    generic:
+        k->variant = FFTZ_VAR_GENERIC;
+        k->nstages = n > 1 ? generic_radices(n, k->radix) : 0;
+        if (k->nstages < 0)
+        {
+            fz_set_error("length %lld has no radix decomposition", (long long)n);
+            return NULL;
+        }
+        k->tpt = k->nstages ? fftz_threads_per_transform(pl->dtype, (int)n, k->nstages, k->radix) : 1;
+        maxthr = fftz_generic_max_threads();
+        if (k->tpt > maxthr)
+        {
+            fz_set_error("length %lld exceeds the generic kernel's thread budget", (long long)n);
+            return NULL;
+        }
+        k->fuse_load = 0;
+        k->fuse_store = 0;
+    }
+    int nslots = (int)n;
+    if (k->nload > nslots) nslots = k->nload;
+    finish_launch_shape(pl, k, nslots, maxthr);
+    if (fftz_pass_smem_bytes(k) > fftz_smem_limit())
+    {
+        fz_set_error("length %lld does not fit shared memory", (long long)n);
+        return NULL;
+    }
+    if (k->nstages > 0)
+    {
+        p->off_tw = fz_stage_twiddles(&pl->blob, pl->dtype, (int)n, k->nstages, k->radix, k->tw_off);
+        if (p->off_tw < 0) return NULL;
+    }
+    snprintf(p->what, sizeof(p->what), "%s n=%lld x%lld", k->variant == FFTZ_VAR_GENERIC ? "generic" : "fast",
+             (long long)n, (long long)k->ntf);
+    return p;
+}
+
+static int single_pass_ok(const fz_plan *pl, int64_t n)
+{
+    if (n == 1) return 1;
+    if (is_pow2(n) && n <= fftz_fast_max_n(pl->dtype)) return 1;
+    int32_t r[FFTZ_MAX_STAGES];
+    int s = generic_radices(n, r);
+    if (s < 0) return 0;
+    int tpt = fftz_threads_per_transform(pl->dtype, (int)n, s, r);
+    if (tpt < 1 || tpt > fftz_generic_max_threads()) return 0;
+    int64_t esz = pl->dtype == 0 ? 8 : 16;
+    return (int64_t)fftz_smem_stride(pl->dtype, (int32_t)n) * esz + 24 <= fftz_smem_limit();
+}
+
+/* n = n1 * n2 with both single-pass lengths; prefers powers of two and a
+ * balanced split with n1 >= n2 (the reference's pow2_balanced_split,
+ * core/common/pow2_radix_decompose.c:15-35) */
+static int choose_split(const fz_plan *pl, int64_t n, int64_t *n1, int64_t *n2)
+{
+    int64_t best1 = 0, best2 = 0;
+    double bestscore = 1e300;
+    for (int64_t a = 2; a * 2 <= n && a <= 1 << 20; a++)
+    {
+        if (n % a) continue;
+        int64_t b = n / a;
+        if (b < 2 || !single_pass_ok(pl, a) || !single_pass_ok(pl, b)) continue;
+        double score = (a > b ? (double)a / b : (double)b / a) + (is_pow2(a) ? 0 : 0.5) + (is_pow2(b) ? 0 : 0.5) +
+                       (a < b ? 0.25 : 0);
+        if (score < bestscore)
+        {
+            bestscore = score;
+            best1 = a;
+            best2 = b;
+        }
+    }
+    if (!best1) return -1;
+    *n1 = best1;
+    *n2 = best2;
+    return 0;
+}
+
+static int64_t lines_of(const fz_dim *b, int nb)
+{
+    int64_t t = 1;
+    for (int i = 0; i < nb; i++) t *= b[i].n;
+    return t;
+}
+
+static void need_scratch(fz_plan *pl, int which, int64_t elems)
+{
+    if (elems > pl->scratch_elems[which]) pl->scratch_elems[which] = elems;
+}
+
+/* Four-step split of one line of length n = n1 * n2 (logical j = n2 j1 + j2,
+ * k = k1 + n1 k2), the reference's pow2 four-step solver
+ * (core/solvers/complex/pow2_fourstep_solver_dft.c:700-763) with its fused
+ * twiddle+transpose (core/kernels/non_dft/fused_twiddle_transpose) folded into
+ * the two passes' stores. */
+static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src, int dst,
+                    int flags)
+{
+    int64_t n1, n2;
+    if (choose_split(pl, n, &n1, &n2)) return -1;
+    int64_t lines = lines_of(b, nb);
+    need_scratch(pl, 0, n * lines);
+    fz_dim bb[FFTZ_MAX_BDIMS + 2];
+    /* pass A: columns j2 of the n1 x n2 view; scratch layout [line][k1][j2] */
+    bb[0].n = n2;
+    bb[0].is = ies;
+    bb[0].os = 1;
+    int64_t so = n;
+    for (int i = 0; i < nb; i++)
+    {
+        bb[i + 1] = b[i];
+        bb[i + 1].os = so;
+        so *= b[i].n;
+    }
+    int64_t L, hi, lo;
+    if (fz_tw4_tables(&pl->blob, n, &L, &hi, &lo)) return -1;
+    fz_pass *pa = line_pass(pl, n1, n2 * ies, n2, bb, nb + 1, 1, src, FZ_BUF_S0,
+                            (flags & FFTZ_F_CONJ_IN) | FFTZ_F_TW4, 0);
+    if (!pa) return -1;
+    pa->k.tw4_n = n;
+    pa->k.tw4_l = L;
+    pa->off_tw4hi = hi;
+    pa->off_tw4lo = lo;
+    /* pass B: rows k1 (contiguous j2) -> X[k1 + n1 k2] */
+    bb[0].n = n1;
+    bb[0].is = n2;
+    bb[0].os = oes;
+    so = n;
+    for (int i = 0; i < nb; i++)
+    {
+        bb[i + 1] = b[i];
+        bb[i + 1].is = so;
+        so *= b[i].n;
+    }
+    fz_pass *pb = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, FZ_BUF_S0, dst, flags & FFTZ_F_CONJ_OUT, 0);
+    if (!pb) return -1;
+    return 0;
+}
+
+/* Bluestein (chirp-z) over a power-of-two m >= 2n - 1 (the reference pads to
+ * a 13-smooth m, core/common/bluestein_utils.c:39-67; a power of two keeps
+ * every sub-transform on the compile-time kernels). */
+static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src, int dst)
+{
+    int64_t m = 1;
+    while (m < 2 * n - 1) m *= 2;
+    int64_t pre, post, mid;
+    if (fz_bluestein_tables(&pl->blob, pl->dtype, n, m, pl->direction, &pre, &post, &mid)) return -1;
+    const int bwd = pl->direction == 1;
+    if (m <= fftz_fast_max_n(pl->dtype) && m >= 4)
+    {
+        fz_pass *p = line_pass(pl, m, ies, oes, b, nb, 0, src, dst,
+                               (bwd ? FFTZ_F_CONJ_IN : FFTZ_F_CONJ_OUT) | FFTZ_F_PRE_TAB | FFTZ_F_POST_TAB |
+                                   FFTZ_F_MID_TAB,
+                               2 | 4);
+        if (!p) return -1;
+        p->k.pre_n = n;
+        p->k.pre_es = 1;
+        p->k.post_n = n;
+        p->k.post_es = 1;
+        p->off_pre = pre;
+        p->off_post = post;
+        p->off_mid = mid;
+        snprintf(p->what, sizeof(p->what), "bluestein n=%lld m=%lld x%lld", (long long)n, (long long)m,
+                 (long long)p->k.ntf);
+        return 0;
+    }
+    /* four passes: FFT_m(pad(x c)) * conj... through S0/S1 */
+    int64_t n1, n2;
+    if (choose_split(pl, m, &n1, &n2)) return -1;
+    int64_t lines = lines_of(b, nb);
+    need_scratch(pl, 0, m * lines);
+    need_scratch(pl, 1, m * lines);
+    int64_t L, hi, lo;
+    if (fz_tw4_tables(&pl->blob, m, &L, &hi, &lo)) return -1;
+    fz_dim bb[FFTZ_MAX_BDIMS + 2];
+    int64_t so;
+    /* A: src -> S0, column FFTs of the padded chirped input */
+    bb[0].n = n2;
+    bb[0].is = ies;
+    bb[0].os = 1;
+    so = m;
+    for (int i = 0; i < nb; i++)
+    {
+        bb[i + 1] = b[i];
+        bb[i + 1].os = so;
+        so *= b[i].n;
+    }
+    fz_pass *pa = line_pass(pl, n1, n2 * ies, n2, bb, nb + 1, 1, src, FZ_BUF_S0,
+                            (bwd ? FFTZ_F_CONJ_IN : 0) | FFTZ_F_PRE_TAB | FFTZ_F_TW4, 2);
+    if (!pa) return -1;
+    pa->k.pre_n = n;
+    pa->k.pre_es = n2;
+    pa->k.pre_cs = 1;
+    pa->k.tw4_n = m;
+    pa->k.tw4_l = L;
+    pa->off_tw4hi = hi;
+    pa->off_tw4lo = lo;
+    pa->off_pre = pre;
+    /* B: S0 -> S1, row FFTs, store conj(A) * conj(Bhat) in natural order */
+    bb[0].n = n1;
+    bb[0].is = n2;
+    bb[0].os = 1;
+    so = m;
+    for (int i = 0; i < nb; i++)
+    {
+        bb[i + 1] = b[i];
+        bb[i + 1].is = so;
+        bb[i + 1].os = so;
+        so *= b[i].n;
+    }
+    fz_pass *pb = line_pass(pl, n2, 1, n1, bb, nb + 1, 1, FZ_BUF_S0, FZ_BUF_S1, FFTZ_F_CONJ_OUT | FFTZ_F_POST_TAB, 2);
+    if (!pb) return -1;
+    pb->k.post_es = n1;
+    pb->k.post_cs = 1;
+    pb->off_post = mid;
+    /* C: S1 -> S0, column FFTs with the four-step twiddle */
+    bb[0].n = n2;
+    bb[0].is = 1;
+    bb[0].os = 1;
+    so = m;
+    for (int i = 0; i < nb; i++)
+    {
+        bb[i + 1] = b[i];
+        bb[i + 1].is = so;
+        bb[i + 1].os = so;
+        so *= b[i].n;
+    }
+    fz_pass *pc = line_pass(pl, n1, n2, n2, bb, nb + 1, 1, FZ_BUF_S1, FZ_BUF_S0, FFTZ_F_TW4, 0);
+    if (!pc) return -1;
+    pc->k.tw4_n = m;
+    pc->k.tw4_l = L;
+    pc->off_tw4hi = hi;
+    pc->off_tw4lo = lo;
+    /* D: S0 -> dst, row FFTs, X_k = chirp_k * conv_k / m for k < n */
+    bb[0].n = n1;
+    bb[0].is = n2;
+    bb[0].os = oes;
+    so = m;
+    for (int i = 0; i < nb; i++)
+    {
+        bb[i + 1] = b[i];
+        bb[i + 1].is = so;
+        so *= b[i].n;
+    }
+    fz_pass *pd = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, FZ_BUF_S0, dst,
+                            (bwd ? 0 : FFTZ_F_CONJ_OUT) | FFTZ_F_POST_TAB, 2);
+    if (!pd) return -1;
+    pd->k.post_n = n;
+    pd->k.post_es = n1;
+    pd->k.post_cs = 1;
+    pd->off_post = post;
+    return 0;
+}
+
+/* one complex line transform of length n over batch b */
+static int add_line(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src, int dst)
+{
+    const int flags = pl->direction ? (FFTZ_F_CONJ_IN | FFTZ_F_CONJ_OUT) : 0;
+    if (n == 1 && src == dst) return 0;
+    if (single_pass_ok(pl, n)) return line_pass(pl, n, ies, oes, b, nb, 0, src, dst, flags, 0) ? 0 : -1;
+    if (smooth13(n) && n <= (int64_t)fftz_fast_max_n(pl->dtype) * fftz_fast_max_n(pl->dtype))
+    {
+        if (src == dst)
+        {
+            /* in place: the four-step reads all of src before the row pass writes dst */
+        }
+        if (fourstep(pl, n, ies, oes, b, nb, src, dst, flags) == 0) return 0;
+    }
+    return bluestein(pl, n, ies, oes, b, nb, src, dst);
+}
+
+/* batch list for the line along dimension d: all other dims, then vecs */
+static int other_dims(const fz_dim *dims, int rank, int d, const fz_dim *vecs, int vrank, fz_dim *out, int use_out)
+{
+    int m = 0;
+    for (int i = 0; i < rank; i++)
+        if (i != d)
+        {
+            out[m] = dims[i];
+            if (use_out) out[m].is = out[m].os;
+            m++;
+        }
+    for (int i = 0; i < vrank; i++)
+    {
+        out[m] = vecs[i];
+        if (use_out) out[m].is = out[m].os;
+        m++;
+    }
+    return m;
+}
+
+static int plan_c2c(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const fz_dim *vecs)
+{
+    fz_dim b[64];
+    for (int d = 0; d < rank; d++)
+    {
+        int first = d == 0;
+        int nb = other_dims(dims, rank, d, vecs, vrank, b, !first);
+        int src = first ? FZ_BUF_IN : FZ_BUF_OUT;
+        int64_t ies = first ? dims[d].is : dims[d].os;
+        if (add_line(pl, dims[d].n, ies, dims[d].os, b, nb, src, FZ_BUF_OUT)) return -1;
+    }
+    return 0;
+}
+
+/* real line along dims[0]: r2c (forward) or c2r (backward) in one generic pass */
+static fz_pass *real_pass(fz_plan *pl, int64_t n0, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src,
+                          int dst)
+{
+    fz_pass *p = push_pass(pl);
+    if (!p) return NULL;
+    fftz_pass_t *k = &p->k;
+    const int packed = (n0 % 2 == 0) && n0 >= 2;
+    const int64_t n = packed ? n0 / 2 : n0;
+    k->n = (int32_t)n;
+    k->ies = ies;
+    k->oes = oes;
+    p->src = src;
+    p->dst = dst;
+    if (pl->direction == 0)
+    {
+        k->in_kind = packed ? FFTZ_IN_REAL_PAIRS : FFTZ_IN_REAL;
+        k->out_kind = packed ? FFTZ_OUT_HALF_RECOMBINE : FFTZ_OUT_HALF;
+        k->nload = (int32_t)n;
+        k->nstore = (int32_t)(n0 / 2 + 1);
+    }
+    else
+    {
+        k->in_kind = packed ? FFTZ_IN_HERM_SEPARATE : FFTZ_IN_HERM_FULL;
+        k->out_kind = packed ? FFTZ_OUT_REAL_PAIRS : FFTZ_OUT_REAL;
+        k->nload = (int32_t)(packed ? n + 1 : n);
+        k->nstore = (int32_t)n;
+        k->flags = packed ? FFTZ_F_CONJ_OUT : FFTZ_F_CONJ_IN;
+    }
+    if (set_batch(k, b, nb, 0)) return NULL;
+    /* element stride of the real side is doubled for pairs */
+    int64_t es_in = (k->in_kind == FFTZ_IN_REAL_PAIRS) ? 2 * ies : ies;
+    int64_t es_out = (k->out_kind == FFTZ_OUT_REAL_PAIRS) ? 2 * oes : oes;
+    k->in_mode = (k->nbdims > 0 && absl(k->ibs[0]) < absl(es_in)) ? 1 : 0;
+    k->out_mode = (k->nbdims > 0 && absl(k->obs[0]) < absl(es_out)) ? 1 : 0;
+    k->variant = FFTZ_VAR_GENERIC;
+    k->nstages = n > 1 ? generic_radices(n, k->radix) : 0;
+    if (k->nstages < 0)
+    {
+        fz_set_error("real length %lld has no radix decomposition", (long long)n0);
+        return NULL;
+    }
+    k->tpt = k->nstages ? fftz_threads_per_transform(pl->dtype, (int)n, k->nstages, k->radix) : 1;
+    if (k->tpt < 1 || k->tpt > fftz_generic_max_threads())
+    {
+        fz_set_error("real length %lld exceeds the one-pass real kernel", (long long)n0);
+        return NULL;
+    }
+    int nslots = k->nload > n ? k->nload : (int)n;
+    finish_launch_shape(pl, k, nslots, fftz_generic_max_threads());
+    if (fftz_pass_smem_bytes(k) > fftz_smem_limit())
+    {
+        fz_set_error("real length %lld does not fit shared memory", (long long)n0);
+        return NULL;
+    }
+    if (k->nstages > 0)
+    {
+        p->off_tw = fz_stage_twiddles(&pl->blob, pl->dtype, (int)n, k->nstages, k->radix, k->tw_off);
+        if (p->off_tw < 0) return NULL;
+    }
+    if (packed)
+    {
+        p->off_rtw = fz_real_twiddles(&pl->blob, pl->dtype, n);
+        if (p->off_rtw < 0) return NULL;
+    }
+    snprintf(p->what, sizeof(p->what), "%s n=%lld x%lld", pl->direction ? "c2r" : "r2c", (long long)n0,
+             (long long)k->ntf);
+    return p;
+}
+
+static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const fz_dim *vecs)
+{
+    const int64_t n0 = dims[0].n;
+    const int64_t h0 = n0 / 2 + 1;
+    fz_dim b[64];
+    if (pl->direction == 0)
+    {
+        /* r2c along dims[0] (real in -> half-complex out), then c2c in place */
+        int nb = other_dims(dims, rank, 0, vecs, vrank, b, 0);
+        if (!real_pass(pl, n0, dims[0].is, dims[0].os, b, nb, FZ_BUF_IN, FZ_BUF_OUT)) return -1;
+        fz_dim hd[16];
+        for (int i = 0; i < rank; i++)
+        {
+            hd[i] = dims[i];
+            hd[i].is = hd[i].os;
+        }
+        hd[0].n = h0;
+        for (int d = 1; d < rank; d++)
+        {
+            int m = other_dims(hd, rank, d, vecs, vrank, b, 1);
+            if (add_line(pl, dims[d].n, dims[d].os, dims[d].os, b, m, FZ_BUF_OUT, FZ_BUF_OUT)) return -1;
+        }
+        return 0;
+    }
+    /* c2r: outer dims first on the half-complex array, then c2r along dims[0].
+     * Out-of-place keeps the input intact: the c2c passes write scratch. */
+    int src = FZ_BUF_IN;
+    fz_dim hd[16];
+    for (int i = 0; i < rank; i++) hd[i] = dims[i];
+    hd[0].n = h0;
+    fz_dim hv[16];
+    for (int i = 0; i < vrank; i++) hv[i] = vecs[i];
+    if (rank > 1)
+    {
+        int work = pl->placement == 0 ? FZ_BUF_IN : FZ_BUF_S1;
+        fz_dim sd[16], sv[16];
+        int64_t st = 1;
+        for (int i = 0; i < rank; i++)
+        {
+            sd[i] = hd[i];
+            if (work == FZ_BUF_S1)
+            {
+                sd[i].os = st;
+                st *= hd[i].n;
+            }
+            else
+                sd[i].os = hd[i].is;
+        }
+        for (int i = 0; i < vrank; i++)
+        {
+            sv[i] = hv[i];
+            if (work == FZ_BUF_S1)
+            {
+                sv[i].os = st;
+                st *= hv[i].n;
+            }
+            else
+                sv[i].os = hv[i].is;
+        }
+        if (work == FZ_BUF_S1) need_scratch(pl, 1, st);
+        for (int d = rank - 1; d >= 1; d--)
+        {
+            int first = d == rank - 1;
+            int m = other_dims(sd, rank, d, sv, vrank, b, !first);
+            int64_t ies = first ? sd[d].is : sd[d].os;
+            if (add_line(pl, dims[d].n, ies, sd[d].os, b, m, first ? FZ_BUF_IN : work, work)) return -1;
+        }
+        src = work;
+        for (int i = 0; i < rank; i++) hd[i].is = sd[i].os;
+        for (int i = 0; i < vrank; i++) hv[i].is = sv[i].os;
+    }
+    int nb = other_dims(hd, rank, 0, hv, vrank, b, 0);
+    return real_pass(pl, n0, hd[0].is, dims[0].os, b, nb, src, FZ_BUF_OUT) ? 0 : -1;
+}
+
+int fz_plan_build(fz_plan *pl, int rank, const fz_dim *dims_in, int vrank, const fz_dim *vecs_in)
+{
+    fz_dim dims[16], vecs[16];
+    int r = 0, v = 0;
+    if (rank > 16 || vrank > 16)
+    {
+        fz_set_error("rank above 16");
+        return -1;
+    }
+    for (int i = 0; i < vrank; i++)
+    {
+        if (vecs_in[i].n == 0) pl->nop = 1;
+        if (vecs_in[i].n != 1) vecs[v++] = vecs_in[i];
+    }
+    if (pl->nop) return 0;
+    if (pl->fft_type == 1)
+    {
+        /* real: dims[0] is the real/half-complex dimension, keep it */
+        dims[r++] = dims_in[0];
+        for (int i = 1; i < rank; i++)
+            if (dims_in[i].n != 1) dims[r++] = dims_in[i];
+        return plan_real(pl, r, dims, v, vecs);
+    }
+    /* drop size-one dims (the reference's SHRINK_DIM_RANK, selector/selector.h:194-214) */
+    for (int i = 0; i < rank; i++)
+        if (dims_in[i].n != 1) dims[r++] = dims_in[i];
+    if (r == 0) dims[r++] = dims_in[0];
+    return plan_c2c(pl, r, dims, v, vecs);
+}

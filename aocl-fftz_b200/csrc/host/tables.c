@@ -1,0 +1,256 @@
+/* Plan-time tables in FP64 (C99 host layer).
+ *
+ * Every twiddle, four-step factor, Bluestein chirp and packed-real twiddle is
+ * formed in double (long double where the argument needs it) from an exactly
+ * reduced integer index, then rounded once to the working precision. The
+ * reference forms its float tables in float (core/common/twiddle.c:24-98) and
+ * only the four-step step twiddles in double
+ * (core/solvers/complex/pow2_fourstep_solver_dft.c:124-171); here every table
+ * is FP64-formed, which is where the stability of a long transform comes from.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "fz_internal.h"
+
+#define FZ_PI_L 3.141592653589793238462643383279502884L
+
+/* exp(-2 pi i r / N) for an exactly reduced 0 <= r < N. The angle is folded
+ * into the first octant so that the long-double cosl/sinl see |x| <= pi/4. */
+static void w_n(int64_t r, int64_t N, double *re, double *im)
+{
+    r %= N;
+    if (r < 0) r += N;
+    /* angle = 2 pi r / N; use 8r/N octants */
+    long double t = (long double)r / (long double)N; /* in [0, 1) turns */
+    long double c, s;
+    long double x = t * 8.0L;
+    int oct = (int)floorl(x);
+    long double f = (x - oct) / 8.0L; /* remaining turns in [0, 1/8) */
+    long double a = 2.0L * FZ_PI_L * f;
+    long double ca = cosl(a), sa = sinl(a);
+    /* exact quarter-turn rotations of (cos a, sin a) */
+    switch (oct & 7)
+    {
+    case 0: c = ca; s = sa; break;
+    case 1: { long double b = 2.0L * FZ_PI_L * (0.125L - f); c = sinl(b); s = cosl(b); break; }
+    case 2: c = -sa; s = ca; break;
+    case 3: { long double b = 2.0L * FZ_PI_L * (0.125L - f); c = -cosl(b); s = sinl(b); break; }
+    case 4: c = -ca; s = -sa; break;
+    case 5: { long double b = 2.0L * FZ_PI_L * (0.125L - f); c = -sinl(b); s = -cosl(b); break; }
+    case 6: c = sa; s = -ca; break;
+    default: { long double b = 2.0L * FZ_PI_L * (0.125L - f); c = cosl(b); s = -sinl(b); break; }
+    }
+    *re = (double)c;
+    *im = (double)(-s);
+}
+
+int64_t fz_blob_reserve(fz_blob *b, size_t bytes)
+{
+    size_t off = (b->len + 255) & ~(size_t)255; /* 256-byte aligned tables */
+    size_t need = off + bytes;
+    if (need > b->cap)
+    {
+        size_t nc = b->cap ? b->cap : 4096;
+        while (nc < need) nc *= 2;
+        unsigned char *np = (unsigned char *)realloc(b->p, nc);
+        if (!np) return -1;
+        b->p = np;
+        b->cap = nc;
+    }
+    memset(b->p + b->len, 0, need - b->len);
+    b->len = need;
+    return (int64_t)off;
+}
+
+int64_t fz_blob_add(fz_blob *b, const void *data, size_t bytes)
+{
+    int64_t off = fz_blob_reserve(b, bytes);
+    if (off >= 0 && bytes) memcpy(b->p + off, data, bytes);
+    return off;
+}
+
+static void put_c(fz_blob *b, int64_t off, int dtype, int64_t idx, double re, double im)
+{
+    if (dtype == 0)
+    {
+        float *f = (float *)(b->p + off);
+        f[2 * idx] = (float)re;
+        f[2 * idx + 1] = (float)im;
+    }
+    else
+    {
+        double *d = (double *)(b->p + off);
+        d[2 * idx] = re;
+        d[2 * idx + 1] = im;
+    }
+}
+
+int64_t fz_stage_twiddles(fz_blob *b, int dtype, int n, int nstages, const int32_t *radix, int32_t *tw_off)
+{
+    /* stage s >= 1 uses W_{Ns*R}^{k*r}, k < Ns, r = 1..R-1, at [(r-1)*Ns + k] */
+    int64_t total = 1, ns = 1;
+    for (int s = 0; s < nstages; s++)
+    {
+        tw_off[s] = (int32_t)total;
+        if (s > 0) total += (int64_t)(radix[s] - 1) * ns;
+        ns *= radix[s];
+    }
+    (void)n;
+    size_t esz = dtype == 0 ? 8 : 16;
+    int64_t off = fz_blob_reserve(b, (size_t)total * esz);
+    if (off < 0) return -1;
+    ns = 1;
+    put_c(b, off, dtype, 0, 1.0, 0.0);
+    for (int s = 0; s < nstages; s++)
+    {
+        int64_t R = radix[s];
+        if (s > 0)
+            for (int64_t r = 1; r < R; r++)
+                for (int64_t k = 0; k < ns; k++)
+                {
+                    double re, im;
+                    w_n(k * r, ns * R, &re, &im);
+                    put_c(b, off, dtype, tw_off[s] + (r - 1) * ns + k, re, im);
+                }
+        ns *= R;
+    }
+    return off;
+}
+
+int fz_tw4_tables(fz_blob *b, int64_t N, int64_t *L, int64_t *off_hi, int64_t *off_lo)
+{
+    int64_t l = 1;
+    while (l * l < N) l *= 2;
+    int64_t nhi = (N + l - 1) / l;
+    *L = l;
+    *off_hi = fz_blob_reserve(b, (size_t)nhi * 16);
+    if (*off_hi < 0) return -1;
+    for (int64_t j = 0; j < nhi; j++)
+    {
+        double re, im;
+        w_n(j * l, N, &re, &im);
+        ((double *)(b->p + *off_hi))[2 * j] = re;
+        ((double *)(b->p + *off_hi))[2 * j + 1] = im;
+    }
+    *off_lo = fz_blob_reserve(b, (size_t)l * 16);
+    if (*off_lo < 0) return -1;
+    for (int64_t j = 0; j < l; j++)
+    {
+        double re, im;
+        w_n(j, N, &re, &im);
+        ((double *)(b->p + *off_lo))[2 * j] = re;
+        ((double *)(b->p + *off_lo))[2 * j + 1] = im;
+    }
+    return 0;
+}
+
+/* in-place iterative radix-2 FFT in double (forward), m a power of two */
+static void host_fft_pow2(double *x, int64_t m)
+{
+    for (int64_t i = 1, j = 0; i < m; i++)
+    {
+        int64_t bit = m >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j)
+        {
+            double t0 = x[2 * i], t1 = x[2 * i + 1];
+            x[2 * i] = x[2 * j];
+            x[2 * i + 1] = x[2 * j + 1];
+            x[2 * j] = t0;
+            x[2 * j + 1] = t1;
+        }
+    }
+    double *w = (double *)malloc(sizeof(double) * (size_t)m);
+    if (!w) return;
+    for (int64_t k = 0; k < m / 2; k++) w_n(k, m, &w[2 * k], &w[2 * k + 1]);
+    for (int64_t len = 2; len <= m; len <<= 1)
+    {
+        int64_t step = m / len;
+        for (int64_t i = 0; i < m; i += len)
+            for (int64_t k = 0; k < len / 2; k++)
+            {
+                double wr = w[2 * k * step], wi = w[2 * k * step + 1];
+                double *a = x + 2 * (i + k), *c = x + 2 * (i + k + len / 2);
+                double tr = c[0] * wr - c[1] * wi, ti = c[0] * wi + c[1] * wr;
+                c[0] = a[0] - tr;
+                c[1] = a[1] - ti;
+                a[0] += tr;
+                a[1] += ti;
+            }
+    }
+    free(w);
+}
+
+int fz_bluestein_tables(fz_blob *b, int dtype, int64_t n, int64_t m, int direction, int64_t *off_pre,
+                        int64_t *off_post, int64_t *off_mid)
+{
+    /* forward chirp c_j = exp(-i pi (j^2 mod 2n) / n) = W_{2n}^{j^2 mod 2n}
+     * (core/common/bluestein_utils.c:88-159 keeps the square exact in integers) */
+    size_t esz = dtype == 0 ? 8 : 16;
+    double *c = (double *)malloc(sizeof(double) * 2 * (size_t)n);
+    double *bb = (double *)calloc(2 * (size_t)m, sizeof(double));
+    if (!c || !bb)
+    {
+        free(c);
+        free(bb);
+        return -1;
+    }
+    const int64_t n2 = 2 * n;
+    for (int64_t j = 0; j < n; j++)
+    {
+        int64_t sq = (int64_t)(((unsigned __int128)j * (unsigned __int128)j) % (unsigned __int128)n2);
+        w_n(sq, n2, &c[2 * j], &c[2 * j + 1]);
+    }
+    /* b_j = conj(c_j) at j and m - j, zero between */
+    for (int64_t j = 0; j < n; j++)
+    {
+        bb[2 * j] = c[2 * j];
+        bb[2 * j + 1] = -c[2 * j + 1];
+        if (j > 0)
+        {
+            bb[2 * (m - j)] = c[2 * j];
+            bb[2 * (m - j) + 1] = -c[2 * j + 1];
+        }
+    }
+    host_fft_pow2(bb, m);
+    *off_pre = fz_blob_reserve(b, (size_t)n * esz);
+    *off_post = fz_blob_reserve(b, (size_t)n * esz);
+    *off_mid = fz_blob_reserve(b, (size_t)m * esz);
+    if (*off_pre < 0 || *off_post < 0 || *off_mid < 0)
+    {
+        free(c);
+        free(bb);
+        return -1;
+    }
+    const double inv_m = 1.0 / (double)m;
+    for (int64_t j = 0; j < n; j++)
+    {
+        put_c(b, *off_pre, dtype, j, c[2 * j], c[2 * j + 1]);
+        if (direction == 0)
+            put_c(b, *off_post, dtype, j, c[2 * j] * inv_m, c[2 * j + 1] * inv_m);
+        else
+            put_c(b, *off_post, dtype, j, c[2 * j] * inv_m, -c[2 * j + 1] * inv_m);
+    }
+    for (int64_t j = 0; j < m; j++) put_c(b, *off_mid, dtype, j, bb[2 * j], -bb[2 * j + 1]);
+    free(c);
+    free(bb);
+    return 0;
+}
+
+int64_t fz_real_twiddles(fz_blob *b, int dtype, int64_t M)
+{
+    size_t esz = dtype == 0 ? 8 : 16;
+    int64_t off = fz_blob_reserve(b, (size_t)(M + 1) * esz);
+    if (off < 0) return -1;
+    for (int64_t k = 0; k < M; k++)
+    {
+        double re, im;
+        w_n(k, 2 * M, &re, &im);
+        put_c(b, off, dtype, k, re, im);
+    }
+    put_c(b, off, dtype, M, -1.0, 0.0);
+    return off;
+}

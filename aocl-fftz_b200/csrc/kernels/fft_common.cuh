@@ -1,0 +1,82 @@
+// Device helpers shared by the shared-memory FFT kernels (generic and
+// compile-time power-of-two families).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "codelets.cuh"
+#include "fftz_kernels.h"
+
+namespace fftz {
+
+template <typename T> struct Cplx;
+template <> struct Cplx<float> {
+  typedef float2 type;
+  enum { PADSH = 4 };  // one pad slot per 16 complex (128 B) of shared memory
+};
+template <> struct Cplx<double> {
+  typedef double2 type;
+  enum { PADSH = 3 };  // one pad slot per 8 complex (128 B)
+};
+
+constexpr int kMaxE = 16;  // complex values a thread holds in one stage
+
+template <typename T2> __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
+  T2 r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+
+template <int SH> __device__ __forceinline__ int phys(int i) { return i + (i >> SH); }
+
+template <typename T2> __device__ __forceinline__ T2 zero2() {
+  T2 z;
+  z.x = 0;
+  z.y = 0;
+  return z;
+}
+
+// W_N^r for r = (col * k) mod N, from two FP64 tables: W = hi[r / L] * lo[r % L].
+template <typename T>
+__device__ __forceinline__ typename Cplx<T>::type tw4(const fftz_pass_t &P, int64_t col, int64_t k) {
+  typedef typename Cplx<T>::type T2;
+  const int64_t N = P.tw4_n, L = P.tw4_l;
+  const int64_t prod = col * k;
+  const int64_t r = ((N & (N - 1)) == 0) ? (prod & (N - 1)) : (prod % N);
+  int64_t hi, lo;
+  if ((L & (L - 1)) == 0) {
+    hi = r >> (63 - __clzll(L));
+    lo = r & (L - 1);
+  } else {
+    hi = r / L;
+    lo = r - hi * L;
+  }
+  const double2 a = __ldg((const double2 *)P.tw4_hi + hi);
+  const double2 b = __ldg((const double2 *)P.tw4_lo + lo);
+  T2 w;
+  w.x = (T)(a.x * b.x - a.y * b.y);
+  w.y = (T)(a.x * b.y + a.y * b.x);
+  return w;
+}
+
+// Epilogue for one complex output element kk of a transform whose column
+// index is col and whose output base offset is obase.
+template <typename T>
+__device__ __forceinline__ void store_complex(const fftz_pass_t &P, typename Cplx<T>::type v, int64_t kk,
+                                              int64_t col, int64_t obase) {
+  typedef typename Cplx<T>::type T2;
+  const int f = P.flags;
+  if (f & FFTZ_F_TW4) v = cmul(v, tw4<T>(P, col, kk));
+  if (f & FFTZ_F_CONJ_OUT) v.y = -v.y;
+  const int64_t li = kk * P.post_es + col * P.post_cs;
+  if (P.post_n > 0 && li >= P.post_n) return;
+  if (f & FFTZ_F_POST_TAB) v = cmul(v, __ldg((const T2 *)P.post_tab + li));
+  if (f & FFTZ_F_SCALE) {
+    v.x = (T)(v.x * P.scale);
+    v.y = (T)(v.y * P.scale);
+  }
+  ((T2 *)P.out)[obase + kk * P.oes] = v;
+}
+
+}  // namespace fftz

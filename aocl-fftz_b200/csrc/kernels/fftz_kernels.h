@@ -1,0 +1,131 @@
+/* Thin C-ABI between the C99 host layer and the sm_100a CUDA kernels.
+ *
+ * The host planner describes every kernel launch as one plain-old-data
+ * fftz_pass_t (no C++ or CUDA types), and calls fftz_launch_pass() with a raw
+ * stream handle. All device pointers are plain void pointers.
+ *
+ * One pass = one launch of the shared-memory FFT kernel: a batch of ntf
+ * transforms of length n, each held whole in shared memory by one CTA
+ * (tf_per_cta transforms per CTA), computed as a sequence of Stockham
+ * radix stages in registers with shared-memory exchanges, with optional fused
+ * prologue (conjugation, chirp / real-pair / Hermitian loads) and epilogue
+ * (four-step twiddle, conjugation, table product, scale, Hermitian
+ * recombination, real stores).
+ */
+#ifndef FFTZ_KERNELS_H
+#define FFTZ_KERNELS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FFTZ_MAX_STAGES 12
+#define FFTZ_MAX_BDIMS 8
+
+/* element kinds of the load phase */
+enum fftz_in_kind {
+    FFTZ_IN_COMPLEX = 0,   /* complex element e at in + base + e*ies           */
+    FFTZ_IN_REAL_PAIRS,    /* (x[2e], x[2e+1]) of a real row, real stride ies   */
+    FFTZ_IN_REAL,          /* (x[e], 0), real stride ies                        */
+    FFTZ_IN_HERM_FULL,     /* e <= n/2 ? X[e] : conj(X[n-e]), complex stride ies */
+    FFTZ_IN_HERM_SEPARATE  /* packed c2r: 2Z[k] from X[k], X[M-k]; k < M        */
+};
+
+/* element kinds of the store phase */
+enum fftz_out_kind {
+    FFTZ_OUT_COMPLEX = 0,  /* complex element k at out + base + k*oes           */
+    FFTZ_OUT_REAL_PAIRS,   /* (out[2k], out[2k+1]) = (re, im), real stride oes   */
+    FFTZ_OUT_REAL,         /* out[k] = re, real stride oes                      */
+    FFTZ_OUT_HALF,         /* first n/2+1 bins of a complex result              */
+    FFTZ_OUT_HALF_RECOMBINE /* packed r2c: X[k], k <= M, from Z[k], Z[M-k]      */
+};
+
+/* kernel families */
+#define FFTZ_VAR_GENERIC 0 /* runtime radix list, any element kind, <= 256 threads   */
+#define FFTZ_VAR_FAST    1 /* compile-time power-of-two shape, complex in/out fused  */
+#define FFTZ_VAR_FAST_TW4 2 /* as FAST with the four-step twiddle epilogue          */
+#define FFTZ_VAR_FAST_TABS 3 /* as FAST with load/store tables, bounds and scale     */
+#define FFTZ_VAR_FAST_TW4_TABS 4 /* both of the above                               */
+#define FFTZ_VAR_FAST_BLUE 5 /* tables plus two sweeps around a mid-table product   */
+
+/* pass flags */
+#define FFTZ_F_CONJ_IN    0x01 /* conjugate each loaded value (after kind decode) */
+#define FFTZ_F_CONJ_OUT   0x02 /* conjugate each stored value (after TW4)         */
+#define FFTZ_F_TW4        0x04 /* multiply output k of column c by W_{tw4_n}^{c*k}  */
+#define FFTZ_F_PRE_TAB    0x08 /* multiply loaded value e by pre_tab[e*pre_es + col*pre_cs] */
+#define FFTZ_F_POST_TAB   0x10 /* multiply stored value k by post_tab[k*post_es + col*post_cs] */
+#define FFTZ_F_SCALE      0x20 /* multiply stored value by scale                  */
+#define FFTZ_F_MID_TAB    0x40 /* two sweeps: between them v = conj(v) * mid_tab[e] */
+
+typedef struct fftz_pass
+{
+    /* transform held in shared memory */
+    int32_t n;                          /* length of the in-SMEM complex transform */
+    int32_t nstages;
+    int32_t radix[FFTZ_MAX_STAGES];
+    int32_t tw_off[FFTZ_MAX_STAGES];    /* stage twiddle block offsets (complex) */
+    int32_t tpt;                        /* threads per transform */
+    int32_t tpc;                        /* transforms per CTA */
+    int32_t sstride;                    /* SMEM complex slots between transforms */
+    int32_t nload;                      /* load-phase element count per transform */
+    int32_t nstore;                     /* store-phase element count per transform */
+    int32_t in_kind, out_kind;
+    int32_t in_mode, out_mode;          /* 0: lanes along elements, 1: along transforms */
+    int32_t flags;
+    int32_t fuse_load, fuse_store;      /* stage 0 reads global / last stage writes global */
+    int32_t variant;                    /* FFTZ_VAR_*: which kernel family runs the pass */
+    int32_t dtype;                      /* 0 float, 1 double */
+    int32_t nbdims;
+    /* addressing: strides in complex elements (real elements for real kinds) */
+    int64_t ies, oes;
+    int64_t ntf;                        /* number of transforms */
+    int64_t bdim[FFTZ_MAX_BDIMS];       /* batch dims, bdim[0] fastest; col = index in bdim[0] */
+    int64_t ibs[FFTZ_MAX_BDIMS];
+    int64_t obs[FFTZ_MAX_BDIMS];
+    /* prologue / epilogue parameters */
+    int64_t tw4_n, tw4_l;               /* W_{tw4_n}^r = hi[r / tw4_l] * lo[r % tw4_l] */
+    int64_t pre_n, pre_es, pre_cs;      /* load bound (0: none) and table index map */
+    int64_t post_n, post_es, post_cs;   /* store bound (0: none) and table index map */
+    double scale;
+    const void *in;
+    void *out;
+    const void *tw;                     /* stage twiddles, working dtype */
+    const void *tw4_hi, *tw4_lo;        /* four-step twiddle factors, double2 */
+    const void *pre_tab, *post_tab, *mid_tab; /* working dtype complex */
+    const void *rtw;                    /* packed-real twiddles W_{2M}^k, working dtype */
+} fftz_pass_t;
+
+/* Largest in-SMEM transform length (complex elements) per dtype. */
+int fftz_max_smem_n(int dtype);
+
+/* Threads per transform of the compile-time power-of-two kernels, and the
+ * largest power-of-two length they cover (0 if none). */
+int fftz_fast_tpt(int n);
+int fftz_fast_max_n(int dtype);
+/* Radix list used by the compile-time kernel for length n (returns stages). */
+int fftz_fast_radices(int n, int32_t *radix);
+/* Threads per CTA the generic kernel may use. */
+int fftz_generic_max_threads(void);
+
+/* Threads-per-transform needed so that no thread holds more than the
+ * register budget in any stage (returns 0 if the plan is not executable). */
+int fftz_threads_per_transform(int dtype, int n, int nstages, const int32_t *radix);
+
+/* Shared memory bytes used by a pass with the given tpc/sstride. */
+int64_t fftz_pass_smem_bytes(const fftz_pass_t *p);
+
+/* Per-transform SMEM stride (complex slots) for nslots elements. */
+int32_t fftz_smem_stride(int dtype, int32_t nslots);
+
+/* Maximum dynamic SMEM bytes per CTA the kernels may use. */
+int64_t fftz_smem_limit(void);
+
+/* Launches one pass on the given stream; returns a cudaError_t value. */
+int fftz_launch_pass(const fftz_pass_t *p, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

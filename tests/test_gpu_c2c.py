@@ -1,0 +1,146 @@
+"""GPU parity of complex transforms, through the C ABI (aoclfftz_setup_* /
+aoclfftz_execute), against the FP64 oracle and the reference library's own
+output on the same seeded inputs.
+
+Bound (written here, used by every case): rel-L2 <= 4 * log2(N) * eps of the
+working dtype, N = product of the transform dims; eps = 2^-23 (f32), 2^-52 (f64).
+Cases follow the reference's test design: every radix and the pow2 iterative,
+four-step, Cooley-Tukey and Bluestein paths (test/bench/CMakeLists.txt:55-124),
+strided and batched layouts, in- and out-of-place, both directions.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from aoclfftz_b200 import synthetic
+from fftz_helpers import cplx_dtype, gather, run_gpu, scatter, span
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_c2c(x, rank, sign):
+    y = np.asarray(x, dtype=np.complex128)
+    for k in range(rank):
+        ax = y.ndim - 1 - k
+        y = np.moveaxis(oracle.fft(np.moveaxis(y, ax, -1), sign=sign), -1, ax)
+    return y
+
+
+def bound(dims, dtype):
+    N = int(np.prod([d[0] for d in dims]))
+    return oracle.tol(N, dtype)
+
+
+def check_c2c(dtype, dims, vecs, direction=0, placement=1, seed=1, host=False, compare_ref=True, ilp64=False):
+    rank = len(dims)
+    lshape = [v[0] for v in reversed(vecs)] + [d[0] for d in reversed(dims)]
+    total = int(np.prod(lshape))
+    x = synthetic.complex_uniform(seed, total, cplx_dtype(dtype)).reshape(lshape)
+    in_sc = 2 * span(dims, vecs, "in")
+    out_sc = 2 * span(dims, vecs, "out")
+    raw_in = scatter(x, [(d[0], d[1]) for d in dims], [(v[0], v[1]) for v in vecs], in_sc, dtype)
+    out_raw, plan = run_gpu(dtype, dims, vecs, raw_in, out_sc, 0, direction, placement, host=host, ilp64=ilp64)
+    y = gather(out_raw, [(d[0], d[2]) for d in dims], [(v[0], v[2]) for v in vecs], dtype)
+    ref = oracle_c2c(x, rank, -1 if direction == 0 else +1)
+    err = oracle.rel_l2(y, ref)
+    assert err <= bound(dims, dtype), "rel-L2 %.3e > %.3e vs FP64 oracle; plan: %s" % (err, bound(dims, dtype), plan)
+    if compare_ref and oracle.ref_available():
+        r_raw = oracle.ref_execute(dtype, dims, vecs, raw_in, out_sc, 0, direction, placement)
+        r = gather(r_raw, [(d[0], d[2]) for d in dims], [(v[0], v[2]) for v in vecs], dtype)
+        # both sides carry rounding error of the working dtype: compare with twice the bound
+        e2 = oracle.rel_l2(y, r)
+        assert e2 <= 2 * bound(dims, dtype), "rel-L2 %.3e vs reference library; plan: %s" % (e2, plan)
+    return err, plan
+
+
+POW2 = [2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192]
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n", POW2)
+@pytest.mark.parametrize("direction", [0, 1])
+def test_pow2_contiguous_batch(dtype, n, direction):
+    b = 3
+    check_c2c(dtype, [(n, 1, 1)], [(b, n, n)], direction)
+
+
+def test_pow2_16384_f32():
+    check_c2c("f32", [(16384, 1, 1)], [(2, 16384, 16384)], 0)
+    check_c2c("f32", [(16384, 1, 1)], [(2, 16384, 16384)], 1)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n", [3, 5, 6, 7, 9, 10, 11, 12, 13, 15, 24, 49, 60, 100, 121, 169, 210, 1000, 1155, 2310])
+def test_mixed_radix(dtype, n):
+    check_c2c(dtype, [(n, 1, 1)], [(4, n, n)], 0)
+    check_c2c(dtype, [(n, 1, 1)], [(2, n, n)], 1)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n", [17, 19, 97, 127, 251, 1009, 4099])
+def test_bluestein_one_kernel(dtype, n):
+    check_c2c(dtype, [(n, 1, 1)], [(3, n, n)], 0)
+    check_c2c(dtype, [(n, 1, 1)], [(2, n, n)], 1)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n", [32768, 65536, 3 ** 10, 2 ** 10 * 3 ** 5])
+def test_fourstep(dtype, n):
+    check_c2c(dtype, [(n, 1, 1)], [(2, n, n)], 0)
+    check_c2c(dtype, [(n, 1, 1)], [(1, n, n)], 1)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+def test_bluestein_multipass(dtype):
+    n = 65521  # largest prime below 2^16: m = 2^17 needs the four-pass form
+    check_c2c(dtype, [(n, 1, 1)], [(1, n, n)], 0)
+    check_c2c(dtype, [(n, 1, 1)], [(1, n, n)], 1)
+
+
+def test_strided_and_inplace():
+    # element stride 3, batch stride 1 (column-major batches), in and out of place
+    n, b = 256, 3
+    check_c2c("f32", [(n, b, b)], [(b, 1, 1)], 0)
+    check_c2c("f64", [(n, b, b)], [(b, 1, 1)], 1, placement=0)
+    check_c2c("f32", [(100, 2, 3)], [(5, 300, 400)], 0)
+    check_c2c("f64", [(64, 1, 1)], [(4, 70, 70)], 0, placement=0)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+def test_multidim(dtype):
+    check_c2c(dtype, [(16, 1, 1), (8, 16, 16)], [(2, 128, 128)], 0)
+    check_c2c(dtype, [(16, 1, 1), (16, 16, 16), (16, 256, 256)], [(1, 4096, 4096)], 1)
+    check_c2c(dtype, [(5, 1, 1), (6, 5, 5), (7, 30, 30)], [(3, 210, 210)], 0)
+    check_c2c(dtype, [(32, 1, 1), (17, 32, 32)], [(2, 544, 544)], 0, placement=0)
+
+
+def test_host_buffers_and_ilp64():
+    check_c2c("f32", [(1024, 1, 1)], [(8, 1024, 1024)], 0, host=True)
+    check_c2c("f64", [(100, 1, 1)], [(3, 100, 100)], 1, host=True, placement=0)
+    check_c2c("f64", [(512, 1, 1)], [(2, 512, 512)], 0, ilp64=True)
+
+
+def test_size_one_and_empty_batch():
+    check_c2c("f32", [(1, 1, 1)], [(5, 1, 1)], 0)
+    check_c2c("f64", [(1, 1, 1), (8, 1, 1)], [(2, 8, 8)], 0)
+
+
+def test_config1_shape():
+    """4096-point fp32 transforms, batch 1024, out of place, forward then backward."""
+    n, b = 4096, 1024
+    check_c2c("f32", [(n, 1, 1)], [(b, n, n)], 0, compare_ref=False)
+    check_c2c("f32", [(n, 1, 1)], [(b, n, n)], 1, compare_ref=False)
+
+
+def test_bit_reproducible():
+    """Ten executions give byte-identical output (the reference's
+    test/test_bit_repro.c procedure, compared with memcmp semantics)."""
+    n = 4096
+    x = synthetic.complex_uniform(7, 16 * n, np.complex64)
+    outs, _ = run_gpu("f32", [(n, 1, 1)], [(16, n, n)], x, 2 * 16 * n, repeat=10)
+    for o in outs[1:]:
+        assert o.tobytes() == outs[0].tobytes()
+    x = synthetic.complex_uniform(8, 4 * 65521, np.complex128)
+    outs, _ = run_gpu("f64", [(65521, 1, 1)], [(4, 65521, 65521)], x, 2 * 4 * 65521, repeat=3)
+    for o in outs[1:]:
+        assert o.tobytes() == outs[0].tobytes()

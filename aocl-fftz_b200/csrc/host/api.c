@@ -28,6 +28,16 @@ void fz_set_error(const char *fmt, ...)
 }
 
 static int g_log_mode = 0;
+static __thread aoclfftz_gpu_hints_t g_hints;
+
+aoclfftz_error_type aoclfftz_gpu_set_hints(const aoclfftz_gpu_hints_t *hints)
+{
+    if (hints)
+        g_hints = *hints;
+    else
+        memset(&g_hints, 0, sizeof(g_hints));
+    return AOCLFFTZ_SUCCESS;
+}
 
 void fz_log(const fz_plan *pl, const char *fmt, ...)
 {
@@ -130,6 +140,12 @@ static void plan_free(fz_plan *pl)
     if (pl->dtab) cudaFree(pl->dtab);
     if (pl->scratch) cudaFree(pl->scratch);
     if (pl->stage) cudaFree(pl->stage);
+    if (pl->prof_ev)
+    {
+        for (int i = 0; i < 2 * pl->prof_cap * pl->npass; i++)
+            if (pl->prof_ev[i]) cudaEventDestroy((cudaEvent_t)pl->prof_ev[i]);
+        free(pl->prof_ev);
+    }
     free(pl->pass);
     free(pl->blob.p);
     pl->magic = 0;
@@ -157,6 +173,7 @@ static void *setup_impl(fz_desc *d, int dtype)
     pl->setup_in = d->in;
     pl->setup_out = d->out;
     pl->stream = NULL;
+    pl->hints = g_hints;
     if (cudaGetDevice(&pl->device) != cudaSuccess)
     {
         fz_set_error("no CUDA device available");
@@ -209,12 +226,13 @@ static void *setup_impl(fz_desc *d, int dtype)
         p->k.post_tab = p->off_post >= 0 ? base + p->off_post : NULL;
         p->k.mid_tab = p->off_mid >= 0 ? base + p->off_mid : NULL;
         p->k.rtw = p->off_rtw >= 0 ? base + p->off_rtw : NULL;
+        if (p->is_elem) p->e.tab = p->off_rtw >= 0 ? base + p->off_rtw : NULL;
     }
     pl->nlaunch = pl->npass;
     const int64_t csz = 2 * esz;
-    int64_t s0 = pl->scratch_elems[0] * csz, s1 = pl->scratch_elems[1] * csz;
-    s0 = (s0 + 255) & ~(int64_t)255;
-    pl->scratch_bytes = s0 + s1;
+    pl->scratch_bytes = 0;
+    for (int i = 0; i < FZ_NSCRATCH; i++)
+        pl->scratch_bytes += (pl->scratch_elems[i] * csz + 255) & ~(int64_t)255;
     if (pl->scratch_bytes > 0 && cudaMalloc(&pl->scratch, (size_t)pl->scratch_bytes) != cudaSuccess)
     {
         cudaGetLastError();
@@ -409,21 +427,45 @@ static aoclfftz_error_type run(fz_plan *pl, void *in, void *out)
         buf[FZ_BUF_IN] = din;
         buf[FZ_BUF_OUT] = dout;
     }
-    int64_t s0 = (pl->scratch_elems[0] * 2 * (pl->dtype == 0 ? 4 : 8) + 255) & ~(int64_t)255;
-    buf[FZ_BUF_S0] = scratch;
-    buf[FZ_BUF_S1] = scratch ? (void *)((unsigned char *)scratch + s0) : NULL;
+    {
+        int64_t off = 0;
+        for (int i = 0; i < FZ_NSCRATCH; i++)
+        {
+            buf[FZ_BUF_S0 + i] = scratch ? (void *)((unsigned char *)scratch + off) : NULL;
+            off += (pl->scratch_elems[i] * 2 * (pl->dtype == 0 ? 4 : 8) + 255) & ~(int64_t)255;
+        }
+    }
     for (int i = 0; i < pl->npass && ret == AOCLFFTZ_SUCCESS; i++)
     {
-        fftz_pass_t k = pl->pass[i].k;
-        k.in = buf[pl->pass[i].src];
-        k.out = buf[pl->pass[i].dst];
-        int e = fftz_launch_pass(&k, st);
+        cudaEvent_t *ev = NULL;
+        if (pl->prof_ev && pl->prof_n < pl->prof_cap)
+        {
+            ev = (cudaEvent_t *)&pl->prof_ev[2 * (pl->prof_n * pl->npass + i)];
+            cudaEventRecord(ev[0], st);
+        }
+        int e;
+        if (pl->pass[i].is_elem)
+        {
+            fftz_elem_t el = pl->pass[i].e;
+            el.in = (const unsigned char *)buf[pl->pass[i].src] + pl->pass[i].in_off;
+            el.out = (unsigned char *)buf[pl->pass[i].dst] + pl->pass[i].out_off;
+            e = fftz_launch_elem(&el, st);
+        }
+        else
+        {
+            fftz_pass_t k = pl->pass[i].k;
+            k.in = (const unsigned char *)buf[pl->pass[i].src] + pl->pass[i].in_off;
+            k.out = (unsigned char *)buf[pl->pass[i].dst] + pl->pass[i].out_off;
+            e = fftz_launch_pass(&k, st);
+        }
+        if (ev) cudaEventRecord(ev[1], st);
         if (e != 0)
         {
             fz_set_error("launch of pass %d (%s) failed: %s", i, pl->pass[i].what, cudaGetErrorString((cudaError_t)e));
             ret = AOCLFFTZ_EXECUTION_FAILURE;
         }
     }
+    if (pl->prof_ev && pl->prof_n < pl->prof_cap) pl->prof_n++;
     if (ret == AOCLFFTZ_SUCCESS && !out_dev)
     {
         if (cudaMemcpyAsync(out, buf[FZ_BUF_OUT], (size_t)pl->out_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -525,8 +567,9 @@ FFTZ_INT32 aoclfftz_gpu_describe(FFTZ_VOID *handle, FFTZ_CHAR *buf, FFTZ_INT32 l
                      pl->direction ? "bwd" : "fwd", pl->placement ? "oop" : "inplace");
     if (pl->nop && w < len) w += snprintf(buf + w, (size_t)(len - w), " empty batch");
     for (int i = 0; i < pl->npass && w < len; i++)
-        w += snprintf(buf + w, (size_t)(len - w), " [%s tpc=%d tpt=%d]", pl->pass[i].what, pl->pass[i].k.tpc,
-                      pl->pass[i].k.tpt);
+        w += pl->pass[i].is_elem ? snprintf(buf + w, (size_t)(len - w), " [%s]", pl->pass[i].what)
+                                  : snprintf(buf + w, (size_t)(len - w), " [%s tpc=%d tpt=%d]", pl->pass[i].what,
+                                             pl->pass[i].k.tpc, pl->pass[i].k.tpt);
     return w < len ? w : len - 1;
 }
 
@@ -535,4 +578,72 @@ FFTZ_INT64 aoclfftz_gpu_device_bytes(FFTZ_VOID *handle)
     fz_plan *pl = as_plan(handle);
     if (!pl) return -1;
     return (FFTZ_INT64)pl->blob.len + pl->scratch_bytes + pl->stage_bytes;
+}
+
+aoclfftz_error_type aoclfftz_gpu_profile_begin(FFTZ_VOID *handle, FFTZ_INT32 max_executes)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl || max_executes <= 0) return AOCLFFTZ_INVALID_INPUT;
+    if (pl->prof_ev)
+    {
+        for (int i = 0; i < 2 * pl->prof_cap * pl->npass; i++)
+            if (pl->prof_ev[i]) cudaEventDestroy((cudaEvent_t)pl->prof_ev[i]);
+        free(pl->prof_ev);
+        pl->prof_ev = NULL;
+    }
+    int n = 2 * max_executes * pl->npass;
+    pl->prof_ev = (void **)calloc((size_t)(n > 0 ? n : 1), sizeof(void *));
+    if (!pl->prof_ev) return AOCLFFTZ_MEMORY_FAILURE;
+    for (int i = 0; i < n; i++)
+        if (cudaEventCreate((cudaEvent_t *)&pl->prof_ev[i]) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return AOCLFFTZ_MEMORY_FAILURE;
+        }
+    pl->prof_cap = max_executes;
+    pl->prof_n = 0;
+    return AOCLFFTZ_SUCCESS;
+}
+
+FFTZ_INT32 aoclfftz_gpu_profile_end(FFTZ_VOID *handle, float *ms_per_pass, FFTZ_INT32 max_passes)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl || !pl->prof_ev) return -1;
+    cudaStreamSynchronize((cudaStream_t)pl->stream);
+    for (int i = 0; i < pl->npass && i < max_passes; i++)
+    {
+        float tot = 0.f;
+        for (int r = 0; r < pl->prof_n; r++)
+        {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, (cudaEvent_t)pl->prof_ev[2 * (r * pl->npass + i)],
+                                 (cudaEvent_t)pl->prof_ev[2 * (r * pl->npass + i) + 1]);
+            tot += ms;
+        }
+        ms_per_pass[i] = tot;
+    }
+    int n = pl->prof_n;
+    for (int i = 0; i < 2 * pl->prof_cap * pl->npass; i++) cudaEventDestroy((cudaEvent_t)pl->prof_ev[i]);
+    free(pl->prof_ev);
+    pl->prof_ev = NULL;
+    pl->prof_cap = pl->prof_n = 0;
+    return n;
+}
+
+FFTZ_INT32 aoclfftz_gpu_pass_info(FFTZ_VOID *handle, FFTZ_INT32 i, FFTZ_CHAR *buf, FFTZ_INT32 len,
+                                  FFTZ_INT64 *elems_in, FFTZ_INT64 *elems_out)
+{
+    fz_plan *pl = as_plan(handle);
+    if (!pl || i < 0 || i >= pl->npass) return -1;
+    const fftz_pass_t *k = &pl->pass[i].k;
+    if (buf && len > 0) snprintf(buf, (size_t)len, "%s", pl->pass[i].what);
+    if (pl->pass[i].is_elem)
+    {
+        if (elems_in) *elems_in = pl->pass[i].e.nlines * pl->pass[i].e.nout;
+        if (elems_out) *elems_out = pl->pass[i].e.nlines * pl->pass[i].e.nout;
+        return pl->npass;
+    }
+    if (elems_in) *elems_in = k->ntf * (int64_t)(k->pre_n > 0 ? k->pre_n : k->nload);
+    if (elems_out) *elems_out = k->ntf * (int64_t)(k->post_n > 0 ? k->post_n : k->nstore);
+    return pl->npass;
 }

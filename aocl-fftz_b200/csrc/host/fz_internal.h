@@ -16,10 +16,15 @@
 
 #include "../kernels/fftz_kernels.h"
 #include "aoclfftz.h"
+#include "aoclfftz_gpu.h"
 
 #define FZ_MAGIC 0x475a4646u /* "FFZG" */
 
-enum { FZ_BUF_IN = 0, FZ_BUF_OUT = 1, FZ_BUF_S0 = 2, FZ_BUF_S1 = 3, FZ_NBUF = 4 };
+/* logical buffers: caller's in / out; S0, S1 used inside multi-pass line
+ * algorithms; W holds the half-complex work array of an out-of-place
+ * multi-dimensional c2r; R holds dense complex lines of a multi-pass real line */
+enum { FZ_BUF_IN = 0, FZ_BUF_OUT = 1, FZ_BUF_S0 = 2, FZ_BUF_S1 = 3, FZ_BUF_W = 4, FZ_BUF_R = 5, FZ_NBUF = 6 };
+#define FZ_NSCRATCH 4
 
 /* one tensor dimension, strides in elements of the side's type */
 typedef struct
@@ -29,8 +34,11 @@ typedef struct
 
 typedef struct
 {
+    int is_elem; /* 0: FFT pass (k), 1: elementwise pass (e) */
+    fftz_elem_t e;
     fftz_pass_t k;
     int src, dst;
+    int64_t in_off, out_off; /* byte offsets added to the src / dst base pointers */
     /* byte offsets of the pass's tables in the plan's table blob (-1: none) */
     int64_t off_tw, off_tw4hi, off_tw4lo, off_pre, off_post, off_mid, off_rtw;
     char what[64];
@@ -57,17 +65,21 @@ typedef struct fz_plan
     int npass, cap;
     fz_pass *pass;
     fz_blob blob;
-    int64_t scratch_elems[2]; /* complex elements of S0, S1 */
+    int64_t scratch_elems[FZ_NSCRATCH]; /* complex elements of S0, S1, W, R */
     /* device state */
     int device;
     void *dtab;
-    void *scratch; /* S0 then S1 in one allocation */
+    void *scratch; /* S0, S1, W, R in one allocation */
     int64_t scratch_bytes;
     void *stage; /* staging buffer for host-memory callers (in, then out) */
     int64_t stage_bytes;
     void *stream; /* cudaStream_t; NULL = legacy default stream */
     int scratch_busy; /* 1 while an execute holds the plan's scratch */
     int nlaunch;
+    aoclfftz_gpu_hints_t hints;
+    /* per-pass event timing: prof_cap executes x npass x {start, end} */
+    void **prof_ev;
+    int prof_cap, prof_n;
 } fz_plan;
 
 /* ---- logging / errors (api.c) ---- */

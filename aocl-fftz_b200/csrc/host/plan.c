@@ -168,6 +168,8 @@ static void finish_launch_shape(fz_plan *pl, fftz_pass_t *k, int nslots, int max
         want = (int)((per + k->n - 1) / k->n);
         if (want * k->tpt < 128) want = (128 + k->tpt - 1) / k->tpt;
     }
+    if ((k->in_mode == 1 || k->out_mode == 1) && pl->hints.tpc_col > 0) want = pl->hints.tpc_col;
+    if (k->in_mode == 0 && k->out_mode == 0 && pl->hints.tpc_row > 0) want = pl->hints.tpc_row;
     int tpc = want;
     if (tpc > by_thr) tpc = by_thr;
     if (tpc > by_smem) tpc = (int)by_smem;
@@ -287,6 +289,13 @@ static int choose_split(const fz_plan *pl, int64_t n, int64_t *n1, int64_t *n2)
 {
     int64_t best1 = 0, best2 = 0;
     double bestscore = 1e300;
+    int64_t h1 = pl->hints.fourstep_n1;
+    if (h1 > 1 && n % h1 == 0 && n / h1 > 1 && single_pass_ok(pl, h1) && single_pass_ok(pl, n / h1))
+    {
+        *n1 = h1;
+        *n2 = n / h1;
+        return 0;
+    }
     for (int64_t a = 2; a * 2 <= n && a <= 1 << 20; a++)
     {
         if (n % a) continue;
@@ -324,13 +333,10 @@ static void need_scratch(fz_plan *pl, int which, int64_t elems)
  * (core/solvers/complex/pow2_fourstep_solver_dft.c:700-763) with its fused
  * twiddle+transpose (core/kernels/non_dft/fused_twiddle_transpose) folded into
  * the two passes' stores. */
-static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src, int dst,
-                    int flags)
+static int fourstep_lines(fz_plan *pl, int64_t n, int64_t n1, int64_t n2, int64_t ies, int64_t oes, const fz_dim *b,
+                          int nb, int src, int dst, int flags, int64_t in_off, int64_t out_off, int64_t hi,
+                          int64_t lo, int64_t L)
 {
-    int64_t n1, n2;
-    if (choose_split(pl, n, &n1, &n2)) return -1;
-    int64_t lines = lines_of(b, nb);
-    need_scratch(pl, 0, n * lines);
     fz_dim bb[FFTZ_MAX_BDIMS + 2];
     /* pass A: columns j2 of the n1 x n2 view; scratch layout [line][k1][j2] */
     bb[0].n = n2;
@@ -343,8 +349,6 @@ static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_d
         bb[i + 1].os = so;
         so *= b[i].n;
     }
-    int64_t L, hi, lo;
-    if (fz_tw4_tables(&pl->blob, n, &L, &hi, &lo)) return -1;
     fz_pass *pa = line_pass(pl, n1, n2 * ies, n2, bb, nb + 1, 1, src, FZ_BUF_S0,
                             (flags & FFTZ_F_CONJ_IN) | FFTZ_F_TW4, 0);
     if (!pa) return -1;
@@ -352,6 +356,7 @@ static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_d
     pa->k.tw4_l = L;
     pa->off_tw4hi = hi;
     pa->off_tw4lo = lo;
+    pa->in_off = in_off;
     /* pass B: rows k1 (contiguous j2) -> X[k1 + n1 k2] */
     bb[0].n = n1;
     bb[0].is = n2;
@@ -365,7 +370,47 @@ static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_d
     }
     fz_pass *pb = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, FZ_BUF_S0, dst, flags & FFTZ_F_CONJ_OUT, 0);
     if (!pb) return -1;
+    pb->out_off = out_off;
     return 0;
+}
+
+/* Four-step split of one line of length n = n1 * n2 (logical j = n2 j1 + j2,
+ * k = k1 + n1 k2), the reference's pow2 four-step solver
+ * (core/solvers/complex/pow2_fourstep_solver_dft.c:700-763) with its fused
+ * twiddle+transpose (core/kernels/non_dft/fused_twiddle_transpose) folded into
+ * the two passes' stores. With a batch chunk, the two passes run per chunk of
+ * lines so that the intermediate of a chunk can stay in L2. */
+static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src, int dst,
+                    int flags)
+{
+    int64_t n1, n2;
+    if (choose_split(pl, n, &n1, &n2)) return -1;
+    int64_t L, hi, lo;
+    if (fz_tw4_tables(&pl->blob, n, &L, &hi, &lo)) return -1;
+    int64_t lines = lines_of(b, nb);
+    int64_t chunk = pl->hints.batch_chunk;
+    int nbig = 0;
+    for (int i = 0; i < nb; i++)
+        if (b[i].n > 1) nbig++;
+    if (chunk > 0 && chunk < lines && nbig == 1)
+    {
+        const int64_t esz = pl->dtype == 0 ? 8 : 16;
+        fz_dim one;
+        for (int i = 0; i < nb; i++)
+            if (b[i].n > 1) one = b[i];
+        need_scratch(pl, 0, n * chunk);
+        for (int64_t c0 = 0; c0 < lines; c0 += chunk)
+        {
+            fz_dim cb = one;
+            cb.n = (lines - c0 < chunk) ? lines - c0 : chunk;
+            if (fourstep_lines(pl, n, n1, n2, ies, oes, &cb, 1, src, dst, flags, c0 * one.is * esz,
+                               c0 * one.os * esz, hi, lo, L))
+                return -1;
+        }
+        return 0;
+    }
+    need_scratch(pl, 0, n * lines);
+    return fourstep_lines(pl, n, n1, n2, ies, oes, b, nb, src, dst, flags, 0, 0, hi, lo, L);
 }
 
 /* Bluestein (chirp-z) over a power-of-two m >= 2n - 1 (the reference pads to
@@ -488,8 +533,11 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
 static int add_line(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src, int dst)
 {
     const int flags = pl->direction ? (FFTZ_F_CONJ_IN | FFTZ_F_CONJ_OUT) : 0;
+    const int algo = pl->hints.algorithm;
     if (n == 1 && src == dst) return 0;
-    if (single_pass_ok(pl, n)) return line_pass(pl, n, ies, oes, b, nb, 0, src, dst, flags, 0) ? 0 : -1;
+    if (algo == 3 && n > 1) return bluestein(pl, n, ies, oes, b, nb, src, dst);
+    if (algo != 2 && single_pass_ok(pl, n))
+        return line_pass(pl, n, ies, oes, b, nb, 0, src, dst, flags, 0) ? 0 : -1;
     if (smooth13(n) && n <= (int64_t)fftz_fast_max_n(pl->dtype) * fftz_fast_max_n(pl->dtype))
     {
         if (src == dst)
@@ -605,6 +653,111 @@ static fz_pass *real_pass(fz_plan *pl, int64_t n0, int64_t ies, int64_t oes, con
     return p;
 }
 
+static int real_pass_ok(const fz_plan *pl, int64_t n0)
+{
+    const int packed = (n0 % 2 == 0) && n0 >= 2;
+    const int64_t n = packed ? n0 / 2 : n0;
+    if (n == 1) return 1;
+    int32_t r[FFTZ_MAX_STAGES];
+    int s = generic_radices(n, r);
+    if (s < 0) return 0;
+    int tpt = fftz_threads_per_transform(pl->dtype, (int)n, s, r);
+    if (tpt < 1 || tpt > fftz_generic_max_threads()) return 0;
+    int64_t esz = pl->dtype == 0 ? 8 : 16;
+    return (int64_t)fftz_smem_stride(pl->dtype, (int32_t)(n + 1)) * esz + 24 <= fftz_smem_limit();
+}
+
+static fz_pass *elem_pass(fz_plan *pl, int mode, int64_t n, int64_t nout, int64_t is, int64_t os, const fz_dim *b,
+                          int nb, int src, int dst)
+{
+    fz_pass *p = push_pass(pl);
+    if (!p) return NULL;
+    p->is_elem = 1;
+    fftz_elem_t *e = &p->e;
+    e->mode = mode;
+    e->dtype = pl->dtype;
+    e->n = n;
+    e->nout = nout;
+    e->is = is;
+    e->os = os;
+    e->nlines = 1;
+    int m = 0;
+    for (int i = 0; i < nb; i++)
+    {
+        if (b[i].n == 1) continue;
+        if (m >= FFTZ_MAX_BDIMS)
+        {
+            fz_set_error("too many batch dimensions for a real line");
+            return NULL;
+        }
+        e->bdim[m] = b[i].n;
+        e->ibs[m] = b[i].is;
+        e->obs[m] = b[i].os;
+        e->nlines *= b[i].n;
+        m++;
+    }
+    e->nbdims = m;
+    p->src = src;
+    p->dst = dst;
+    static const char *names[] = {"widen", "widen-pairs", "recombine", "separate", "herm-expand", "narrow-half",
+                                  "real-out", "pairs-out"};
+    snprintf(p->what, sizeof(p->what), "elem %s n=%lld x%lld", names[mode], (long long)n, (long long)e->nlines);
+    return p;
+}
+
+/* Real line of length n0 along dims[0] that one CTA cannot hold: widen into a
+ * dense complex scratch line (R), run any complex line algorithm on it, then
+ * recombine / narrow into the destination. Packed (even n0) lines use the
+ * n0/2-point complex transform as the reference's packed solver does. */
+static int real_line_multipass(fz_plan *pl, int64_t n0, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src,
+                               int dst)
+{
+    const int packed = (n0 % 2 == 0);
+    const int64_t len = packed ? n0 / 2 : n0;
+    fz_dim side_in[32], side_out[32], dense[32];
+    int64_t ds = len;
+    for (int i = 0; i < nb; i++)
+    {
+        dense[i] = b[i];
+        dense[i].is = dense[i].os = ds;
+        ds *= b[i].n;
+        side_in[i] = b[i];
+        side_in[i].os = dense[i].os;
+        side_out[i] = b[i];
+        side_out[i].is = dense[i].is;
+    }
+    need_scratch(pl, 3, ds);
+    int64_t rtw = -1;
+    if (packed && (rtw = fz_real_twiddles(&pl->blob, pl->dtype, len)) < 0) return -1;
+    fz_pass *p;
+    if (pl->direction == 0)
+    {
+        p = elem_pass(pl, packed ? FFTZ_ELEM_WIDEN_PAIRS : FFTZ_ELEM_WIDEN_REAL, len, len, ies, 1, side_in, nb, src,
+                      FZ_BUF_R);
+        if (!p) return -1;
+        if (add_line(pl, len, 1, 1, dense, nb, FZ_BUF_R, FZ_BUF_R)) return -1;
+        p = elem_pass(pl, packed ? FFTZ_ELEM_RECOMBINE : FFTZ_ELEM_NARROW_HALF, len, n0 / 2 + 1, 1, oes, side_out, nb,
+                      FZ_BUF_R, dst);
+        if (!p) return -1;
+        p->off_rtw = rtw;
+        return 0;
+    }
+    p = elem_pass(pl, packed ? FFTZ_ELEM_SEPARATE : FFTZ_ELEM_HERM_EXPAND, len, len, ies, 1, side_in, nb, src,
+                  FZ_BUF_R);
+    if (!p) return -1;
+    p->off_rtw = rtw;
+    if (add_line(pl, len, 1, 1, dense, nb, FZ_BUF_R, FZ_BUF_R)) return -1;
+    p = elem_pass(pl, packed ? FFTZ_ELEM_PAIRS_OUT : FFTZ_ELEM_REAL_OUT, len, len, 1, oes, side_out, nb, FZ_BUF_R,
+                  dst);
+    return p ? 0 : -1;
+}
+
+static int real_line(fz_plan *pl, int64_t n0, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src, int dst)
+{
+    if (real_pass_ok(pl, n0)) return real_pass(pl, n0, ies, oes, b, nb, src, dst) ? 0 : -1;
+    return real_line_multipass(pl, n0, ies, oes, b, nb, src, dst);
+}
+
 static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const fz_dim *vecs)
 {
     const int64_t n0 = dims[0].n;
@@ -614,7 +767,7 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
     {
         /* r2c along dims[0] (real in -> half-complex out), then c2c in place */
         int nb = other_dims(dims, rank, 0, vecs, vrank, b, 0);
-        if (!real_pass(pl, n0, dims[0].is, dims[0].os, b, nb, FZ_BUF_IN, FZ_BUF_OUT)) return -1;
+        if (real_line(pl, n0, dims[0].is, dims[0].os, b, nb, FZ_BUF_IN, FZ_BUF_OUT)) return -1;
         fz_dim hd[16];
         for (int i = 0; i < rank; i++)
         {
@@ -630,7 +783,7 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
         return 0;
     }
     /* c2r: outer dims first on the half-complex array, then c2r along dims[0].
-     * Out-of-place keeps the input intact: the c2c passes write scratch. */
+     * Out-of-place keeps the input intact: the c2c passes work in scratch W. */
     int src = FZ_BUF_IN;
     fz_dim hd[16];
     for (int i = 0; i < rank; i++) hd[i] = dims[i];
@@ -639,13 +792,13 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
     for (int i = 0; i < vrank; i++) hv[i] = vecs[i];
     if (rank > 1)
     {
-        int work = pl->placement == 0 ? FZ_BUF_IN : FZ_BUF_S1;
+        int work = pl->placement == 0 ? FZ_BUF_IN : FZ_BUF_W;
         fz_dim sd[16], sv[16];
         int64_t st = 1;
         for (int i = 0; i < rank; i++)
         {
             sd[i] = hd[i];
-            if (work == FZ_BUF_S1)
+            if (work == FZ_BUF_W)
             {
                 sd[i].os = st;
                 st *= hd[i].n;
@@ -656,7 +809,7 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
         for (int i = 0; i < vrank; i++)
         {
             sv[i] = hv[i];
-            if (work == FZ_BUF_S1)
+            if (work == FZ_BUF_W)
             {
                 sv[i].os = st;
                 st *= hv[i].n;
@@ -664,7 +817,7 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
             else
                 sv[i].os = hv[i].is;
         }
-        if (work == FZ_BUF_S1) need_scratch(pl, 1, st);
+        if (work == FZ_BUF_W) need_scratch(pl, 2, st);
         for (int d = rank - 1; d >= 1; d--)
         {
             int first = d == rank - 1;
@@ -677,7 +830,7 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
         for (int i = 0; i < vrank; i++) hv[i].is = sv[i].os;
     }
     int nb = other_dims(hd, rank, 0, hv, vrank, b, 0);
-    return real_pass(pl, n0, hd[0].is, dims[0].os, b, nb, src, FZ_BUF_OUT) ? 0 : -1;
+    return real_line(pl, n0, hd[0].is, dims[0].os, b, nb, src, FZ_BUF_OUT);
 }
 
 int fz_plan_build(fz_plan *pl, int rank, const fz_dim *dims_in, int vrank, const fz_dim *vecs_in)

@@ -97,6 +97,33 @@ typedef struct fftz_pass
     const void *rtw;                    /* packed-real twiddles W_{2M}^k, working dtype */
 } fftz_pass_t;
 
+/* Elementwise real-transform helpers (fft_elem.cu) */
+enum fftz_elem_mode {
+    FFTZ_ELEM_WIDEN_REAL = 0,
+    FFTZ_ELEM_WIDEN_PAIRS,
+    FFTZ_ELEM_RECOMBINE,
+    FFTZ_ELEM_SEPARATE,
+    FFTZ_ELEM_HERM_EXPAND,
+    FFTZ_ELEM_NARROW_HALF,
+    FFTZ_ELEM_REAL_OUT,
+    FFTZ_ELEM_PAIRS_OUT
+};
+
+typedef struct fftz_elem
+{
+    int32_t mode, dtype, nbdims, pad_;
+    int64_t n;      /* line length parameter of the mode (n, or M for packed) */
+    int64_t nout;   /* outputs per line */
+    int64_t nlines;
+    int64_t is, os; /* element strides on the input / output side */
+    int64_t bdim[FFTZ_MAX_BDIMS], ibs[FFTZ_MAX_BDIMS], obs[FFTZ_MAX_BDIMS];
+    const void *in;
+    void *out;
+    const void *tab; /* packed-real twiddles W_{2M}^k, k <= M */
+} fftz_elem_t;
+
+int fftz_launch_elem(const fftz_elem_t *e, void *stream);
+
 /* Largest in-SMEM transform length (complex elements) per dtype. */
 int fftz_max_smem_n(int dtype);
 

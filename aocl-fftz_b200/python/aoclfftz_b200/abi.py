@@ -51,6 +51,12 @@ DescLP64 = _desc(Dim)     # aoclfftz_prob_desc_f / _d
 DescILP64 = _desc(Dim64)  # aoclfftz_prob_desc_f_64_ / _d_64_
 
 
+class Hints(C.Structure):
+    """aoclfftz_gpu_hints_t (include/aoclfftz_gpu.h)."""
+    _fields_ = [("fourstep_n1", C.c_int64), ("tpc_col", C.c_int32), ("tpc_row", C.c_int32),
+                ("batch_chunk", C.c_int64), ("algorithm", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
 def bind(lib):
     """Declares the aoclfftz.h prototypes on a loaded shared object."""
     for name, desc in (("aoclfftz_setup_f", DescLP64), ("aoclfftz_setup_d", DescLP64),
@@ -84,6 +90,15 @@ def bind_gpu(lib):
     lib.aoclfftz_gpu_describe.restype = C.c_int32
     lib.aoclfftz_gpu_device_bytes.argtypes = [C.c_void_p]
     lib.aoclfftz_gpu_device_bytes.restype = C.c_int64
+    lib.aoclfftz_gpu_profile_begin.argtypes = [C.c_void_p, C.c_int32]
+    lib.aoclfftz_gpu_profile_begin.restype = C.c_int
+    lib.aoclfftz_gpu_profile_end.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int32]
+    lib.aoclfftz_gpu_profile_end.restype = C.c_int32
+    lib.aoclfftz_gpu_pass_info.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_int64),
+                                           C.POINTER(C.c_int64)]
+    lib.aoclfftz_gpu_pass_info.restype = C.c_int32
+    lib.aoclfftz_gpu_set_hints.argtypes = [C.c_void_p]
+    lib.aoclfftz_gpu_set_hints.restype = C.c_int
     lib.aoclfftz_gpu_last_error.argtypes = []
     lib.aoclfftz_gpu_last_error.restype = C.c_char_p
     return lib

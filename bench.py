@@ -1,0 +1,414 @@
+#!/usr/bin/env python3
+"""Benchmark of the FFT plan-execution path on B200.
+
+Default workload (one step = forward then backward, unnormalised):
+  c2c fp32, N = 2^24 = 4096 x 4096 (four-step: two passes through HBM),
+  batch 4, out of place; inputs re, im i.i.d. U[-1, 1) from a seed.
+Other workloads (--workload): "batch4096" (N = 4096, batch 1024, one pass).
+
+Metric: 5 N log2(N) GFLOP/s over all transforms of the step (both directions),
+plus HBM GB/s. `value` is measured with inputs resident in HBM; `e2e` runs the
+same step through the public C ABI with pinned host buffers (the library
+stages them: copy in, transform, copy out). `roofline` describes the dominant
+kernel, timed with CUDA events on the plan's stream during the timed region.
+`cpu_baseline` times the reference library (built from its sources, OpenMP)
+on a bounded sample on this host's cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU (torchrun, one process per GPU): every rank runs its own batch
+(weak scaling, no collective on the data path); the time is the max over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "aocl-fftz_b200", "python"))
+
+WORKLOADS = {
+    "fourstep24": dict(n=1 << 24, batch=4, dtype="f32",
+                       desc="c2c fp32 N=2^24 (4096x4096 four-step) batch 4, out-of-place, fwd+bwd"),
+    "batch4096": dict(n=4096, batch=1024, dtype="f32",
+                      desc="c2c fp32 N=4096 batch 1024, out-of-place, fwd+bwd"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="fourstep24", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def make_plan(lib, abi, pin, pout, n, batch, direction, dtype):
+    desc, keep = abi.make_desc(pin, pout, [(n, 1, 1)], [(batch, n, n)], 0, direction, 1)
+    h = abi.setup(lib, desc, dtype)
+    if not h:
+        raise RuntimeError("setup failed: %s" % lib.aoclfftz_gpu_last_error().decode())
+    return h
+
+
+def pass_table(lib, h):
+    out = []
+    k = lib.aoclfftz_gpu_num_launches(h)
+    for i in range(k):
+        buf = C.create_string_buffer(128)
+        ei, eo = C.c_int64(), C.c_int64()
+        lib.aoclfftz_gpu_pass_info(h, i, buf, 128, C.byref(ei), C.byref(eo))
+        out.append((buf.value.decode(), ei.value, eo.value))
+    return out
+
+
+def run_ours(args, wl):
+    import numpy as np
+    import torch
+
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi, synthetic
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    lib = aoclfftz_b200.load()
+    n, b, dtype = wl["n"], wl["batch"], wl["dtype"]
+    esz = 8 if dtype == "f32" else 16
+    total = n * b
+    x = synthetic.complex_uniform(1234 + rank, total, np.complex64 if dtype == "f32" else np.complex128)
+    real = x.view(np.float32 if dtype == "f32" else np.float64)
+    hx = torch.from_numpy(real).pin_memory()
+    dx = hx.to("cuda")
+    dy = torch.empty_like(dx)
+    dz = torch.empty_like(dx)
+    stream = torch.cuda.Stream()
+    pf = make_plan(lib, abi, dx.data_ptr(), dy.data_ptr(), n, b, 0, dtype)
+    pb = make_plan(lib, abi, dy.data_ptr(), dz.data_ptr(), n, b, 1, dtype)
+    for h in (pf, pb):
+        lib.aoclfftz_gpu_set_stream(h, C.c_void_p(stream.cuda_stream))
+
+    def step():
+        if lib.aoclfftz_execute(pf) or lib.aoclfftz_execute(pb):
+            raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    torch.cuda.synchronize()
+    # correctness of the round trip on this run's data: z = N x
+    zc = dz.view(torch.complex64 if dtype == "f32" else torch.complex128)
+    xc = dx.view(zc.dtype)
+    rt_err = (torch.linalg.vector_norm(zc / n - xc) / torch.linalg.vector_norm(xc)).item()
+
+    K = args.steps
+    lib.aoclfftz_gpu_profile_begin(pf, K)
+    lib.aoclfftz_gpu_profile_begin(pb, K)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(K):
+            step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    npf, npb = lib.aoclfftz_gpu_num_launches(pf), lib.aoclfftz_gpu_num_launches(pb)
+    tf = (C.c_float * 16)()
+    tb = (C.c_float * 16)()
+    lib.aoclfftz_gpu_profile_end(pf, tf, 16)
+    lib.aoclfftz_gpu_profile_end(pb, tb, 16)
+    if ws > 1:
+        t = torch.tensor([ms_total], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms = ms_total / K
+    flops_step = 2 * b * 5.0 * n * math.log2(n) * ws
+    value = flops_step / (ms * 1e-3) / 1e9
+    alg_bytes_step = 2 * b * n * 2 * esz * ws  # each direction reads and writes the batch once
+    hbm_gbs = alg_bytes_step / (ms * 1e-3) / 1e9
+
+    # dominant kernel: the pass with the largest summed time
+    passes = [("fwd",) + p for p in pass_table(lib, pf)] + [("bwd",) + p for p in pass_table(lib, pb)]
+    times = [tf[i] for i in range(npf)] + [tb[i] for i in range(npb)]
+    dom = max(range(len(times)), key=lambda i: times[i])
+    dom_ms = times[dom] / K
+    dom_bytes = (passes[dom][2] + passes[dom][3]) * esz
+    peak, peak_kind = load_peaks()
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    res = dict(ms=ms, value=value, hbm_gbs=hbm_gbs, rt_err=rt_err, clocks=clk, launches=K * (npf + npb),
+               roofline={"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "kernel": "%s %s" % (passes[dom][0], passes[dom][1]),
+                         "bytes_per_launch": dom_bytes, "ms_per_launch": round(dom_ms, 5),
+                         "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
+                         else "fallback 6650 GB/s"},
+               passes=[{"pass": "%s %s" % (p[0], p[1]), "ms": round(t / K, 5),
+                        "GB/s": round((p[2] + p[3]) * esz / (t / K * 1e-3) / 1e9, 1)}
+                       for p, t in zip(passes, times)])
+
+    # end to end through the C ABI with pinned host buffers
+    if not args.no_e2e:
+        hy = torch.empty_like(hx).pin_memory()
+        hz = torch.empty_like(hx).pin_memory()
+        qf = make_plan(lib, abi, hx.data_ptr(), hy.data_ptr(), n, b, 0, dtype)
+        qb = make_plan(lib, abi, hy.data_ptr(), hz.data_ptr(), n, b, 1, dtype)
+        for h in (qf, qb):
+            lib.aoclfftz_gpu_set_stream(h, C.c_void_p(stream.cuda_stream))
+
+        def estep():
+            if lib.aoclfftz_execute(qf) or lib.aoclfftz_execute(qb):
+                raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
+
+        for _ in range(2):
+            estep()
+        KE = max(3, min(K, 10))
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(KE):
+            estep()
+        torch.cuda.synchronize()
+        e_ms = (time.perf_counter() - t0) * 1e3 / KE
+        if ws > 1:
+            t = torch.tensor([e_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e_ms = float(t.item())
+        ez = hz.numpy().view(x.dtype)
+        e_err = float(np.linalg.norm(ez / n - x) / np.linalg.norm(x))
+        res["e2e"] = {"value": round(flops_step / (e_ms * 1e-3) / 1e9, 2), "unit": "GFLOP/s",
+                      "h2d_bytes_per_step": 2 * b * n * esz, "d2h_bytes_per_step": 2 * b * n * esz,
+                      "ms_per_step": round(e_ms, 3), "steps": KE, "round_trip_rel_l2": e_err,
+                      "api": "aoclfftz_execute with pinned host in/out (library stages H2D, FFT, D2H)"}
+        lib.aoclfftz_destroy(qf)
+        lib.aoclfftz_destroy(qb)
+    lib.aoclfftz_destroy(pf)
+    lib.aoclfftz_destroy(pb)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return res
+
+
+def time_reference(wl, threads, transforms, steps, warmup, min_time=None):
+    """The reference library's own CPU path (AOCL-FFTZ compiled from its
+    sources into oracle/_ref/, OpenMP) through aoclfftz_setup_f/execute on host
+    buffers. One step = forward then backward of `transforms` transforms.
+    Returns (seconds per step, steps timed)."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from aoclfftz_b200 import abi, synthetic
+
+    L = oracle.ref_lib()
+    n, dtype = wl["n"], wl["dtype"]
+    cd = np.complex64 if dtype == "f32" else np.complex128
+    x = synthetic.complex_uniform(99, n * transforms, cd)
+    y = np.empty_like(x)
+    z = np.empty_like(x)
+    plans = []
+    for (a, b_, d) in ((x, y, 0), (y, z, 1)):
+        desc, keep = abi.make_desc(a.ctypes.data, b_.ctypes.data, [(n, 1, 1)], [(transforms, n, n)], 0, d, 1,
+                                   num_threads=threads, opt_level=3)
+        h = abi.setup(L, desc, dtype)
+        if not h:
+            raise RuntimeError("reference setup failed")
+        plans.append(h)
+
+    def step():
+        for h in plans:
+            if L.aoclfftz_execute(h) != 0:
+                raise RuntimeError("reference execute failed")
+
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        step()
+        k += 1
+        el = time.perf_counter() - t0
+        if steps is not None and k >= steps:
+            break
+        if steps is None and el >= min_time:
+            break
+    for h in plans:
+        L.aoclfftz_destroy(h)
+    err = float(np.linalg.norm(z / n - x) / np.linalg.norm(x))
+    return el / k, k, err
+
+
+def flops_per_transform(n):
+    return 2 * 5.0 * n * math.log2(n)  # forward + backward
+
+
+def cpu_baseline(wl):
+    threads = os.cpu_count() or 1
+    n = wl["n"]
+    t = max(1, min(wl["batch"], (1 << 22) // n)) if n < (1 << 22) else 1
+    sec, k, err = time_reference(wl, threads, t, None, 1, min_time=10.0)
+    return {"value": round(flops_per_transform(n) * t / sec / 1e9, 3), "unit": "GFLOP/s", "cores": threads,
+            "kind": "reference",
+            "sample": "%d x %d-point %s c2c fwd+bwd per rep, %d reps (%.1f s), OpenMP %d threads, opt_level 3"
+                      % (t, n, wl["dtype"], k, sec * k, threads),
+            "round_trip_rel_l2": err}
+
+
+def run_reference(args, wl):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "reference library not built (oracle/_ref/libaocl_fftz.so)"}
+    threads = os.cpu_count() or 1
+    n = wl["n"]
+    t = wl["batch"]
+    sec1, _, _ = time_reference(wl, threads, t, 1, 0)
+    if sec1 * (args.steps + args.warmup) > 150:
+        t = max(1, int(t * 150 / (sec1 * (args.steps + args.warmup))))
+    sec, k, err = time_reference(wl, threads, t, args.steps, args.warmup)
+    v = flops_per_transform(n) * t / sec / 1e9
+    base = {"metric": METRIC, "value": round(v, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": wl["dtype"], "data": "synthetic (splitmix64 U[-1,1))", "impl": "reference",
+            "config": {"workload": wl["desc"], "n": n, "batch": wl["batch"], "sample_transforms_per_step": t},
+            "cpu_baseline": {"value": round(v, 3), "unit": "GFLOP/s", "cores": threads, "kind": "reference",
+                             "sample": "%d of %d transforms per step, fwd+bwd, OpenMP %d threads" % (t, wl["batch"],
+                                                                                                 threads)},
+            "e2e": {"value": round(v, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "round_trip_rel_l2": err}
+    return base
+
+
+METRIC = "5N·log2N GFLOP/s + HBM GB/s vs plain GPU FFT at stated FP64 err, 1 B200"
+
+
+def main():
+    args = parse()
+    wl = WORKLOADS[args.workload]
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        out = run_reference(args, wl)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    r = run_ours(args, wl)
+    if rank != 0:
+        return
+    peak, peak_kind = load_peaks()
+    line = {"metric": METRIC, "value": round(r["value"], 2), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(r["ms"], 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": wl["dtype"], "data": "synthetic (splitmix64 U[-1,1))",
+            "config": {"workload": wl["desc"], "n": wl["n"], "batch_per_gpu": wl["batch"],
+                       "global_batch": wl["batch"] * ws, "l2": "inputs larger than L2 (no flush needed)"
+                       if wl["n"] * wl["batch"] * 8 > 126e6 else "inputs fit L2",
+                       "parallelism": "replicas dp%d" % ws},
+            "hbm_gbs": round(r["hbm_gbs"], 1), "hbm_frac_of_measured": round(r["hbm_gbs"] / peak, 4),
+            "roofline": r["roofline"], "gpu_launches": r["launches"], "clocks": r["clocks"],
+            "round_trip_rel_l2": r["rt_err"], "passes": r["passes"]}
+    if "e2e" in r:
+        line["e2e"] = r["e2e"]
+    if ws == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(wl)
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -34,6 +34,40 @@ FFTZ_INT32 aoclfftz_gpu_describe(FFTZ_VOID *handle, FFTZ_CHAR *buf, FFTZ_INT32 l
 /* Device bytes the plan owns (tables, scratch, staging). */
 FFTZ_INT64 aoclfftz_gpu_device_bytes(FFTZ_VOID *handle);
 
+/* Per-pass timing with CUDA events recorded around every launch on the plan's
+ * stream (no synchronisation between executes). profile_begin arms it for up
+ * to max_executes executes; profile_end synchronises the stream, writes the
+ * summed milliseconds of each pass into ms_per_pass and returns the number of
+ * executes recorded. */
+aoclfftz_error_type aoclfftz_gpu_profile_begin(FFTZ_VOID *handle, FFTZ_INT32 max_executes);
+FFTZ_INT32 aoclfftz_gpu_profile_end(FFTZ_VOID *handle, float *ms_per_pass, FFTZ_INT32 max_passes);
+
+/* Pass i of the plan: description, complex (or real-pair) elements read and
+ * written per launch. Returns the number of passes, -1 on a bad index. */
+FFTZ_INT32 aoclfftz_gpu_pass_info(FFTZ_VOID *handle, FFTZ_INT32 i, FFTZ_CHAR *buf, FFTZ_INT32 len,
+                                  FFTZ_INT64 *elems_in, FFTZ_INT64 *elems_out);
+
+/* Planner hints for the next aoclfftz_setup_* calls made by this thread
+ * (the autotuner's knobs). Zero in a field means "planner's choice".
+ *   fourstep_n1   column length n1 of a four-step split n = n1 * n2
+ *   tpc_col       transforms per CTA for passes with column-mapped lanes
+ *   tpc_row       transforms per CTA for row passes
+ *   batch_chunk   multi-pass plans run their passes on chunks of this many
+ *                 lines at a time (keeps the intermediate resident in L2)
+ *   algorithm     1 one pass, 2 four-step, 3 Bluestein (0 = choose)
+ * aoclfftz_gpu_set_hints(NULL) restores the defaults. */
+typedef struct aoclfftz_gpu_hints
+{
+    FFTZ_INT64 fourstep_n1;
+    FFTZ_INT32 tpc_col;
+    FFTZ_INT32 tpc_row;
+    FFTZ_INT64 batch_chunk;
+    FFTZ_INT32 algorithm;
+    FFTZ_INT32 reserved[7];
+} aoclfftz_gpu_hints_t;
+
+aoclfftz_error_type aoclfftz_gpu_set_hints(const aoclfftz_gpu_hints_t *hints);
+
 /* Text of the last error recorded by this thread (empty if none). */
 const FFTZ_CHAR *aoclfftz_gpu_last_error(FFTZ_VOID);
 

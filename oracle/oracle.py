@@ -124,8 +124,12 @@ def fft_nd(x, sign=-1):
 
 
 def rfft_packed(x):
+    """r2c along the last axis: packed restatement for even n, full complex
+    transform of the real input (first n/2+1 bins) for odd n."""
     x = np.ascontiguousarray(x, dtype=np.float64)
     n = x.shape[-1]
+    if n % 2:
+        return fft(x.astype(np.complex128))[..., : n // 2 + 1]
     out = np.empty(x.shape[:-1] + (n // 2 + 1,), dtype=np.complex128)
     xs, os_ = x.reshape(-1, n), out.reshape(-1, n // 2 + 1)
     for i in range(xs.shape[0]):
@@ -135,7 +139,15 @@ def rfft_packed(x):
 
 
 def irfft_packed(X, n):
+    """c2r along the last axis (unnormalised): packed restatement for even n,
+    Hermitian completion and a full complex transform for odd n."""
     X = _c128(X)
+    if n % 2:
+        full = np.empty(X.shape[:-1] + (n,), dtype=np.complex128)
+        h = n // 2 + 1
+        full[..., :h] = X[..., :h]
+        full[..., h:] = np.conj(X[..., 1:n - h + 1][..., ::-1])
+        return fft(full, sign=+1).real.copy()
     out = np.empty(X.shape[:-1] + (n,), dtype=np.float64)
     xs, os_ = X.reshape(-1, X.shape[-1]), out.reshape(-1, n)
     for i in range(xs.shape[0]):
@@ -144,19 +156,22 @@ def irfft_packed(X, n):
     return out
 
 
-def rfftn(x):
-    """Real N-D forward transform: packed r2c along the last axis, then exact
-    complex transforms along the others (what the reference's packed 3-D path
-    computes, core/solvers/real/packed_solver_rdft.c:154-186)."""
+def rfftn(x, rank=None):
+    """Real N-D forward transform over the last `rank` axes (all by default):
+    packed r2c along the last axis, then complex transforms along the others
+    (what the reference's packed 3-D path computes,
+    core/solvers/real/packed_solver_rdft.c:154-186)."""
+    rank = x.ndim if rank is None else rank
     h = rfft_packed(x)
-    for ax in range(x.ndim - 1):
+    for ax in range(x.ndim - rank, x.ndim - 1):
         h = np.moveaxis(fft(np.moveaxis(h, ax, -1)), -1, ax)
     return h
 
 
-def irfftn(X, n_last):
+def irfftn(X, n_last, rank=None):
+    rank = X.ndim if rank is None else rank
     h = _c128(X)
-    for ax in range(X.ndim - 1):
+    for ax in range(X.ndim - rank, X.ndim - 1):
         h = np.moveaxis(fft(np.moveaxis(h, ax, -1), sign=+1), -1, ax)
     return irfft_packed(h, n_last)
 

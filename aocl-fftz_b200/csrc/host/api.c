@@ -231,7 +231,7 @@ static void *setup_impl(fz_desc *d, int dtype)
     pl->nlaunch = pl->npass;
     const int64_t csz = 2 * esz;
     pl->scratch_bytes = 0;
-    for (int i = 0; i < FZ_NSCRATCH; i++)
+    for (int i = 0; i < pl->nscratch; i++)
         pl->scratch_bytes += (pl->scratch_elems[i] * csz + 255) & ~(int64_t)255;
     if (pl->scratch_bytes > 0 && cudaMalloc(&pl->scratch, (size_t)pl->scratch_bytes) != cudaSuccess)
     {
@@ -429,9 +429,9 @@ static aoclfftz_error_type run(fz_plan *pl, void *in, void *out)
     }
     {
         int64_t off = 0;
-        for (int i = 0; i < FZ_NSCRATCH; i++)
+        for (int i = 0; i < pl->nscratch; i++)
         {
-            buf[FZ_BUF_S0 + i] = scratch ? (void *)((unsigned char *)scratch + off) : NULL;
+            buf[FZ_BUF_SCR0 + i] = scratch ? (void *)((unsigned char *)scratch + off) : NULL;
             off += (pl->scratch_elems[i] * 2 * (pl->dtype == 0 ? 4 : 8) + 255) & ~(int64_t)255;
         }
     }

@@ -20,11 +20,13 @@
 
 #define FZ_MAGIC 0x475a4646u /* "FFZG" */
 
-/* logical buffers: caller's in / out; S0, S1 used inside multi-pass line
- * algorithms; W holds the half-complex work array of an out-of-place
- * multi-dimensional c2r; R holds dense complex lines of a multi-pass real line */
-enum { FZ_BUF_IN = 0, FZ_BUF_OUT = 1, FZ_BUF_S0 = 2, FZ_BUF_S1 = 3, FZ_BUF_W = 4, FZ_BUF_R = 5, FZ_NBUF = 6 };
-#define FZ_NSCRATCH 4
+/* logical buffers: the caller's in / out, then plan-owned scratch arrays,
+ * one per use (four-step intermediates, Bluestein work arrays, the
+ * half-complex work array of an out-of-place multi-dimensional c2r, dense
+ * lines of a multi-pass real line) */
+enum { FZ_BUF_IN = 0, FZ_BUF_OUT = 1, FZ_BUF_SCR0 = 2 };
+#define FZ_MAX_SCRATCH 16
+#define FZ_NBUF (FZ_BUF_SCR0 + FZ_MAX_SCRATCH)
 
 /* one tensor dimension, strides in elements of the side's type */
 typedef struct
@@ -65,11 +67,13 @@ typedef struct fz_plan
     int npass, cap;
     fz_pass *pass;
     fz_blob blob;
-    int64_t scratch_elems[FZ_NSCRATCH]; /* complex elements of S0, S1, W, R */
+    int64_t scratch_elems[FZ_MAX_SCRATCH]; /* complex elements of each scratch array */
+    int nscratch;
+    int depth; /* planner recursion depth (hints apply at depth 0) */
     /* device state */
     int device;
     void *dtab;
-    void *scratch; /* S0, S1, W, R in one allocation */
+    void *scratch; /* all scratch arrays in one allocation */
     int64_t scratch_bytes;
     void *stage; /* staging buffer for host-memory callers (in, then out) */
     int64_t stage_bytes;
@@ -91,8 +95,8 @@ int64_t fz_blob_add(fz_blob *b, const void *data, size_t bytes);
 int64_t fz_blob_reserve(fz_blob *b, size_t bytes);
 /* stage twiddles for a radix list; returns blob offset, fills tw_off[] */
 int64_t fz_stage_twiddles(fz_blob *b, int dtype, int n, int nstages, const int32_t *radix, int32_t *tw_off);
-/* four-step factor tables W_N^(hi*L), W_N^lo as double2 */
-int fz_tw4_tables(fz_blob *b, int64_t N, int64_t *L, int64_t *off_hi, int64_t *off_lo);
+/* four-step factor tables W_N^(hi*L), W_N^lo in the working dtype */
+int fz_tw4_tables(fz_blob *b, int dtype, int64_t N, int64_t *L, int64_t *off_hi, int64_t *off_lo);
 /* Bluestein tables for length n, pow2 convolution length m, direction */
 int fz_bluestein_tables(fz_blob *b, int dtype, int64_t n, int64_t m, int direction, int64_t *off_pre,
                         int64_t *off_post, int64_t *off_mid);

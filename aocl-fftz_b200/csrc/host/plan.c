@@ -151,25 +151,31 @@ static int set_batch(fftz_pass_t *k, const fz_dim *b, int nb, int keep_first)
 }
 
 /* transforms per CTA: enough columns for coalesced column access, enough
- * work per CTA for short rows, bounded by threads and shared memory */
+ * work per CTA for short rows, bounded by threads and shared memory (two
+ * slots for the double-buffered kernels) */
+static int is_pipe_variant(int v) { return v == FFTZ_VAR_PIPE || v == FFTZ_VAR_PIPE_TW4; }
+
 static void finish_launch_shape(fz_plan *pl, fftz_pass_t *k, int nslots, int maxthr)
 {
     const int64_t esz = pl->dtype == 0 ? 8 : 16;
+    const int pipe = is_pipe_variant(k->variant);
+    const int colmap = (k->in_mode == 1 || k->out_mode == 1);
     k->sstride = fftz_smem_stride(pl->dtype, nslots);
     int by_thr = maxthr / k->tpt;
     if (by_thr < 1) by_thr = 1;
-    int64_t by_smem = fftz_smem_limit() / ((int64_t)k->sstride * esz + 24);
+    const int64_t per_tf = (pipe ? 2 : 1) * ((int64_t)k->sstride + 16) * esz + (pipe ? 72 : 24);
+    int64_t by_smem = fftz_smem_limit() / per_tf;
     int want;
-    if (k->in_mode == 1 || k->out_mode == 1)
-        want = pl->dtype == 0 ? 8 : 4; /* 64-byte column segments */
+    if (colmap)
+        want = pipe ? 2 : (pl->dtype == 0 ? 8 : 4); /* column segments */
     else
     {
-        int64_t per = pl->dtype == 0 ? 4096 : 2048; /* complex elements per CTA */
+        int64_t per = pipe ? 4096 : (pl->dtype == 0 ? 4096 : 2048); /* complex elements per CTA */
         want = (int)((per + k->n - 1) / k->n);
         if (want * k->tpt < 128) want = (128 + k->tpt - 1) / k->tpt;
     }
-    if ((k->in_mode == 1 || k->out_mode == 1) && pl->hints.tpc_col > 0) want = pl->hints.tpc_col;
-    if (k->in_mode == 0 && k->out_mode == 0 && pl->hints.tpc_row > 0) want = pl->hints.tpc_row;
+    if (colmap && pl->hints.tpc_col > 0) want = pl->hints.tpc_col;
+    if (!colmap && pl->hints.tpc_row > 0) want = pl->hints.tpc_row;
     int tpc = want;
     if (tpc > by_thr) tpc = by_thr;
     if (tpc > by_smem) tpc = (int)by_smem;
@@ -177,6 +183,7 @@ static void finish_launch_shape(fz_plan *pl, fftz_pass_t *k, int nslots, int max
     if (tpc > 1024) tpc = 1024;
     if (tpc < 1) tpc = 1;
     k->tpc = tpc;
+    if (colmap) k->sstride = fftz_smem_stride_cols(pl->dtype, nslots, tpc);
 }
 
 static void set_modes(fftz_pass_t *k)
@@ -213,7 +220,15 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         maxthr = pl->dtype == 0 ? 1024 : 512;
         if (k->nstages == 1 && k->in_mode != k->out_mode) k->out_mode = k->in_mode;
         int tabs = (variant_bits & 2) != 0, tw4 = (flags & FFTZ_F_TW4) != 0;
-        if (variant_bits & 4)
+        const int fam = pl->hints.kernel_family;
+        const int pipe_ok = n >= 64 && !tabs && !(variant_bits & 4);
+        /* the persistent double-buffered kernel is a tuning option (hint
+         * kernel_family = 2); measured on B200 the one-tile-per-CTA kernel is
+         * faster for both dtypes and both lane maps, so it is the default */
+        const int pipe_default = 0;
+        if (pipe_ok && (fam == 2 || (fam == 0 && pipe_default)))
+            k->variant = tw4 ? FFTZ_VAR_PIPE_TW4 : FFTZ_VAR_PIPE;
+        else if (variant_bits & 4)
             k->variant = FFTZ_VAR_FAST_BLUE;
         else if (tabs && tw4)
             k->variant = FFTZ_VAR_FAST_TW4_TABS;
@@ -228,6 +243,7 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
             /* small feature kernels are not instantiated: use the generic one */
             goto generic;
         }
+        if (is_pipe_variant(k->variant)) maxthr = fftz_pipe_max_threads((int)n);
         k->fuse_load = 1;
         k->fuse_store = 1;
     }
@@ -254,6 +270,13 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
     int nslots = (int)n;
     if (k->nload > nslots) nslots = k->nload;
     finish_launch_shape(pl, k, nslots, maxthr);
+    if (is_pipe_variant(k->variant) && fftz_pass_smem_bytes(k) > fftz_smem_limit())
+    {
+        /* two slots do not fit: the one-tile-per-CTA kernel of the same shape */
+        k->variant = k->variant == FFTZ_VAR_PIPE_TW4 ? FFTZ_VAR_FAST_TW4 : FFTZ_VAR_FAST;
+        maxthr = pl->dtype == 0 ? 1024 : 512;
+        finish_launch_shape(pl, k, nslots, maxthr);
+    }
     if (fftz_pass_smem_bytes(k) > fftz_smem_limit())
     {
         fz_set_error("length %lld does not fit shared memory", (long long)n);
@@ -264,7 +287,8 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         p->off_tw = fz_stage_twiddles(&pl->blob, pl->dtype, (int)n, k->nstages, k->radix, k->tw_off);
         if (p->off_tw < 0) return NULL;
     }
-    snprintf(p->what, sizeof(p->what), "%s n=%lld x%lld", k->variant == FFTZ_VAR_GENERIC ? "generic" : "fast",
+    snprintf(p->what, sizeof(p->what), "%s n=%lld x%lld",
+             k->variant == FFTZ_VAR_GENERIC ? "generic" : (is_pipe_variant(k->variant) ? "pipe" : "fast"),
              (long long)n, (long long)k->ntf);
     return p;
 }
@@ -285,12 +309,18 @@ static int single_pass_ok(const fz_plan *pl, int64_t n)
 /* n = n1 * n2 with both single-pass lengths; prefers powers of two and a
  * balanced split with n1 >= n2 (the reference's pow2_balanced_split,
  * core/common/pow2_radix_decompose.c:15-35) */
+static int splittable(const fz_plan *pl, int64_t n)
+{
+    const int64_t m = fftz_fast_max_n(pl->dtype);
+    return single_pass_ok(pl, n) || (smooth13(n) && n <= m * m);
+}
+
 static int choose_split(const fz_plan *pl, int64_t n, int64_t *n1, int64_t *n2)
 {
     int64_t best1 = 0, best2 = 0;
     double bestscore = 1e300;
-    int64_t h1 = pl->hints.fourstep_n1;
-    if (h1 > 1 && n % h1 == 0 && n / h1 > 1 && single_pass_ok(pl, h1) && single_pass_ok(pl, n / h1))
+    int64_t h1 = pl->depth == 0 ? pl->hints.fourstep_n1 : 0;
+    if (h1 > 1 && n % h1 == 0 && n / h1 > 1 && single_pass_ok(pl, h1) && splittable(pl, n / h1))
     {
         *n1 = h1;
         *n2 = n / h1;
@@ -323,9 +353,17 @@ static int64_t lines_of(const fz_dim *b, int nb)
     return t;
 }
 
-static void need_scratch(fz_plan *pl, int which, int64_t elems)
+/* a new plan-owned scratch array of elems complex elements; returns its
+ * buffer id, or -1 when the plan already holds the maximum number */
+static int new_scratch(fz_plan *pl, int64_t elems)
 {
-    if (elems > pl->scratch_elems[which]) pl->scratch_elems[which] = elems;
+    if (pl->nscratch >= FZ_MAX_SCRATCH)
+    {
+        fz_set_error("plan needs more than %d scratch arrays", FZ_MAX_SCRATCH);
+        return -1;
+    }
+    pl->scratch_elems[pl->nscratch] = elems;
+    return FZ_BUF_SCR0 + pl->nscratch++;
 }
 
 /* Four-step split of one line of length n = n1 * n2 (logical j = n2 j1 + j2,
@@ -333,9 +371,12 @@ static void need_scratch(fz_plan *pl, int which, int64_t elems)
  * (core/solvers/complex/pow2_fourstep_solver_dft.c:700-763) with its fused
  * twiddle+transpose (core/kernels/non_dft/fused_twiddle_transpose) folded into
  * the two passes' stores. */
+static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_dim *b, int nb, int src, int dst,
+                    int flags);
+
 static int fourstep_lines(fz_plan *pl, int64_t n, int64_t n1, int64_t n2, int64_t ies, int64_t oes, const fz_dim *b,
                           int nb, int src, int dst, int flags, int64_t in_off, int64_t out_off, int64_t hi,
-                          int64_t lo, int64_t L)
+                          int64_t lo, int64_t L, int S)
 {
     fz_dim bb[FFTZ_MAX_BDIMS + 2];
     /* pass A: columns j2 of the n1 x n2 view; scratch layout [line][k1][j2] */
@@ -349,8 +390,7 @@ static int fourstep_lines(fz_plan *pl, int64_t n, int64_t n1, int64_t n2, int64_
         bb[i + 1].os = so;
         so *= b[i].n;
     }
-    fz_pass *pa = line_pass(pl, n1, n2 * ies, n2, bb, nb + 1, 1, src, FZ_BUF_S0,
-                            (flags & FFTZ_F_CONJ_IN) | FFTZ_F_TW4, 0);
+    fz_pass *pa = line_pass(pl, n1, n2 * ies, n2, bb, nb + 1, 1, src, S, (flags & FFTZ_F_CONJ_IN) | FFTZ_F_TW4, 0);
     if (!pa) return -1;
     pa->k.tw4_n = n;
     pa->k.tw4_l = L;
@@ -368,7 +408,16 @@ static int fourstep_lines(fz_plan *pl, int64_t n, int64_t n1, int64_t n2, int64_
         bb[i + 1].is = so;
         so *= b[i].n;
     }
-    fz_pass *pb = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, FZ_BUF_S0, dst, flags & FFTZ_F_CONJ_OUT, 0);
+    if (!single_pass_ok(pl, n2))
+    {
+        /* the rows are themselves split: a nested four-step over length n2 */
+        if (out_off) return -1;
+        pl->depth++;
+        int rc = fourstep(pl, n2, 1, n1 * oes, bb, nb + 1, S, dst, flags & FFTZ_F_CONJ_OUT);
+        pl->depth--;
+        return rc;
+    }
+    fz_pass *pb = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, S, dst, flags & FFTZ_F_CONJ_OUT, 0);
     if (!pb) return -1;
     pb->out_off = out_off;
     return 0;
@@ -386,7 +435,7 @@ static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_d
     int64_t n1, n2;
     if (choose_split(pl, n, &n1, &n2)) return -1;
     int64_t L, hi, lo;
-    if (fz_tw4_tables(&pl->blob, n, &L, &hi, &lo)) return -1;
+    if (fz_tw4_tables(&pl->blob, pl->dtype, n, &L, &hi, &lo)) return -1;
     int64_t lines = lines_of(b, nb);
     int64_t chunk = pl->hints.batch_chunk;
     int nbig = 0;
@@ -398,19 +447,21 @@ static int fourstep(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_d
         fz_dim one;
         for (int i = 0; i < nb; i++)
             if (b[i].n > 1) one = b[i];
-        need_scratch(pl, 0, n * chunk);
+        int S = new_scratch(pl, n * chunk);
+        if (S < 0 || !single_pass_ok(pl, n2)) return -1;
         for (int64_t c0 = 0; c0 < lines; c0 += chunk)
         {
             fz_dim cb = one;
             cb.n = (lines - c0 < chunk) ? lines - c0 : chunk;
             if (fourstep_lines(pl, n, n1, n2, ies, oes, &cb, 1, src, dst, flags, c0 * one.is * esz,
-                               c0 * one.os * esz, hi, lo, L))
+                               c0 * one.os * esz, hi, lo, L, S))
                 return -1;
         }
         return 0;
     }
-    need_scratch(pl, 0, n * lines);
-    return fourstep_lines(pl, n, n1, n2, ies, oes, b, nb, src, dst, flags, 0, 0, hi, lo, L);
+    int S = new_scratch(pl, n * lines);
+    if (S < 0) return -1;
+    return fourstep_lines(pl, n, n1, n2, ies, oes, b, nb, src, dst, flags, 0, 0, hi, lo, L, S);
 }
 
 /* Bluestein (chirp-z) over a power-of-two m >= 2n - 1 (the reference pads to
@@ -445,10 +496,10 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
     int64_t n1, n2;
     if (choose_split(pl, m, &n1, &n2)) return -1;
     int64_t lines = lines_of(b, nb);
-    need_scratch(pl, 0, m * lines);
-    need_scratch(pl, 1, m * lines);
+    const int S0 = new_scratch(pl, m * lines), S1 = new_scratch(pl, m * lines);
+    if (S0 < 0 || S1 < 0) return -1;
     int64_t L, hi, lo;
-    if (fz_tw4_tables(&pl->blob, m, &L, &hi, &lo)) return -1;
+    if (fz_tw4_tables(&pl->blob, pl->dtype, m, &L, &hi, &lo)) return -1;
     fz_dim bb[FFTZ_MAX_BDIMS + 2];
     int64_t so;
     /* A: src -> S0, column FFTs of the padded chirped input */
@@ -462,7 +513,7 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
         bb[i + 1].os = so;
         so *= b[i].n;
     }
-    fz_pass *pa = line_pass(pl, n1, n2 * ies, n2, bb, nb + 1, 1, src, FZ_BUF_S0,
+    fz_pass *pa = line_pass(pl, n1, n2 * ies, n2, bb, nb + 1, 1, src, S0,
                             (bwd ? FFTZ_F_CONJ_IN : 0) | FFTZ_F_PRE_TAB | FFTZ_F_TW4, 2);
     if (!pa) return -1;
     pa->k.pre_n = n;
@@ -485,7 +536,7 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
         bb[i + 1].os = so;
         so *= b[i].n;
     }
-    fz_pass *pb = line_pass(pl, n2, 1, n1, bb, nb + 1, 1, FZ_BUF_S0, FZ_BUF_S1, FFTZ_F_CONJ_OUT | FFTZ_F_POST_TAB, 2);
+    fz_pass *pb = line_pass(pl, n2, 1, n1, bb, nb + 1, 1, S0, S1, FFTZ_F_CONJ_OUT | FFTZ_F_POST_TAB, 2);
     if (!pb) return -1;
     pb->k.post_es = n1;
     pb->k.post_cs = 1;
@@ -502,7 +553,7 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
         bb[i + 1].os = so;
         so *= b[i].n;
     }
-    fz_pass *pc = line_pass(pl, n1, n2, n2, bb, nb + 1, 1, FZ_BUF_S1, FZ_BUF_S0, FFTZ_F_TW4, 0);
+    fz_pass *pc = line_pass(pl, n1, n2, n2, bb, nb + 1, 1, S1, S0, FFTZ_F_TW4, 0);
     if (!pc) return -1;
     pc->k.tw4_n = m;
     pc->k.tw4_l = L;
@@ -519,7 +570,7 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
         bb[i + 1].is = so;
         so *= b[i].n;
     }
-    fz_pass *pd = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, FZ_BUF_S0, dst,
+    fz_pass *pd = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, S0, dst,
                             (bwd ? 0 : FFTZ_F_CONJ_OUT) | FFTZ_F_POST_TAB, 2);
     if (!pd) return -1;
     pd->k.post_n = n;
@@ -726,28 +777,29 @@ static int real_line_multipass(fz_plan *pl, int64_t n0, int64_t ies, int64_t oes
         side_out[i] = b[i];
         side_out[i].is = dense[i].is;
     }
-    need_scratch(pl, 3, ds);
+    const int RB = new_scratch(pl, ds);
+    if (RB < 0) return -1;
     int64_t rtw = -1;
     if (packed && (rtw = fz_real_twiddles(&pl->blob, pl->dtype, len)) < 0) return -1;
     fz_pass *p;
     if (pl->direction == 0)
     {
         p = elem_pass(pl, packed ? FFTZ_ELEM_WIDEN_PAIRS : FFTZ_ELEM_WIDEN_REAL, len, len, ies, 1, side_in, nb, src,
-                      FZ_BUF_R);
+                      RB);
         if (!p) return -1;
-        if (add_line(pl, len, 1, 1, dense, nb, FZ_BUF_R, FZ_BUF_R)) return -1;
+        if (add_line(pl, len, 1, 1, dense, nb, RB, RB)) return -1;
         p = elem_pass(pl, packed ? FFTZ_ELEM_RECOMBINE : FFTZ_ELEM_NARROW_HALF, len, n0 / 2 + 1, 1, oes, side_out, nb,
-                      FZ_BUF_R, dst);
+                      RB, dst);
         if (!p) return -1;
         p->off_rtw = rtw;
         return 0;
     }
     p = elem_pass(pl, packed ? FFTZ_ELEM_SEPARATE : FFTZ_ELEM_HERM_EXPAND, len, len, ies, 1, side_in, nb, src,
-                  FZ_BUF_R);
+                  RB);
     if (!p) return -1;
     p->off_rtw = rtw;
-    if (add_line(pl, len, 1, 1, dense, nb, FZ_BUF_R, FZ_BUF_R)) return -1;
-    p = elem_pass(pl, packed ? FFTZ_ELEM_PAIRS_OUT : FFTZ_ELEM_REAL_OUT, len, len, 1, oes, side_out, nb, FZ_BUF_R,
+    if (add_line(pl, len, 1, 1, dense, nb, RB, RB)) return -1;
+    p = elem_pass(pl, packed ? FFTZ_ELEM_PAIRS_OUT : FFTZ_ELEM_REAL_OUT, len, len, 1, oes, side_out, nb, RB,
                   dst);
     return p ? 0 : -1;
 }
@@ -792,13 +844,21 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
     for (int i = 0; i < vrank; i++) hv[i] = vecs[i];
     if (rank > 1)
     {
-        int work = pl->placement == 0 ? FZ_BUF_IN : FZ_BUF_W;
+        int work = FZ_BUF_IN;
+        if (pl->placement != 0)
+        {
+            int64_t tot = 1;
+            for (int i = 0; i < rank; i++) tot *= hd[i].n;
+            for (int i = 0; i < vrank; i++) tot *= hv[i].n;
+            work = new_scratch(pl, tot);
+            if (work < 0) return -1;
+        }
         fz_dim sd[16], sv[16];
         int64_t st = 1;
         for (int i = 0; i < rank; i++)
         {
             sd[i] = hd[i];
-            if (work == FZ_BUF_W)
+            if (work != FZ_BUF_IN)
             {
                 sd[i].os = st;
                 st *= hd[i].n;
@@ -809,7 +869,7 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
         for (int i = 0; i < vrank; i++)
         {
             sv[i] = hv[i];
-            if (work == FZ_BUF_W)
+            if (work != FZ_BUF_IN)
             {
                 sv[i].os = st;
                 st *= hv[i].n;
@@ -817,7 +877,6 @@ static int plan_real(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const
             else
                 sv[i].os = hv[i].is;
         }
-        if (work == FZ_BUF_W) need_scratch(pl, 2, st);
         for (int d = rank - 1; d >= 1; d--)
         {
             int first = d == rank - 1;

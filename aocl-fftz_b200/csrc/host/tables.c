@@ -119,29 +119,30 @@ int64_t fz_stage_twiddles(fz_blob *b, int dtype, int n, int nstages, const int32
     return off;
 }
 
-int fz_tw4_tables(fz_blob *b, int64_t N, int64_t *L, int64_t *off_hi, int64_t *off_lo)
+int fz_tw4_tables(fz_blob *b, int dtype, int64_t N, int64_t *L, int64_t *off_hi, int64_t *off_lo)
 {
+    /* W_N^r = hi[r / L] * lo[r % L]: both factors formed in FP64 and stored in
+     * the working precision (the product is taken in the working precision) */
     int64_t l = 1;
     while (l * l < N) l *= 2;
     int64_t nhi = (N + l - 1) / l;
+    size_t esz = dtype == 0 ? 8 : 16;
     *L = l;
-    *off_hi = fz_blob_reserve(b, (size_t)nhi * 16);
+    *off_hi = fz_blob_reserve(b, (size_t)nhi * esz);
     if (*off_hi < 0) return -1;
     for (int64_t j = 0; j < nhi; j++)
     {
         double re, im;
         w_n(j * l, N, &re, &im);
-        ((double *)(b->p + *off_hi))[2 * j] = re;
-        ((double *)(b->p + *off_hi))[2 * j + 1] = im;
+        put_c(b, *off_hi, dtype, j, re, im);
     }
-    *off_lo = fz_blob_reserve(b, (size_t)l * 16);
+    *off_lo = fz_blob_reserve(b, (size_t)l * esz);
     if (*off_lo < 0) return -1;
     for (int64_t j = 0; j < l; j++)
     {
         double re, im;
         w_n(j, N, &re, &im);
-        ((double *)(b->p + *off_lo))[2 * j] = re;
-        ((double *)(b->p + *off_lo))[2 * j + 1] = im;
+        put_c(b, *off_lo, dtype, j, re, im);
     }
     return 0;
 }

@@ -37,27 +37,24 @@ template <typename T2> __device__ __forceinline__ T2 zero2() {
   return z;
 }
 
-// W_N^r for r = (col * k) mod N, from two FP64 tables: W = hi[r / L] * lo[r % L].
+// W_N^r for r = (col * k) mod N from two tables (factors formed in FP64, held
+// in the working precision): W = hi[r / L] * lo[r % L]. Powers of two take a
+// 32-bit path (r = col * k mod 2^32 reduced mod N is exact for N <= 2^31).
 template <typename T>
 __device__ __forceinline__ typename Cplx<T>::type tw4(const fftz_pass_t &P, int64_t col, int64_t k) {
   typedef typename Cplx<T>::type T2;
   const int64_t N = P.tw4_n, L = P.tw4_l;
-  const int64_t prod = col * k;
-  const int64_t r = ((N & (N - 1)) == 0) ? (prod & (N - 1)) : (prod % N);
   int64_t hi, lo;
-  if ((L & (L - 1)) == 0) {
-    hi = r >> (63 - __clzll(L));
-    lo = r & (L - 1);
+  if (((N & (N - 1)) == 0) && N <= 0x80000000LL && ((L & (L - 1)) == 0)) {
+    const unsigned r = ((unsigned)col * (unsigned)k) & (unsigned)(N - 1);
+    hi = r >> (31 - __clz((int)L));
+    lo = r & (unsigned)(L - 1);
   } else {
+    const int64_t r = (col * k) % N;
     hi = r / L;
     lo = r - hi * L;
   }
-  const double2 a = __ldg((const double2 *)P.tw4_hi + hi);
-  const double2 b = __ldg((const double2 *)P.tw4_lo + lo);
-  T2 w;
-  w.x = (T)(a.x * b.x - a.y * b.y);
-  w.y = (T)(a.x * b.y + a.y * b.x);
-  return w;
+  return cmul(__ldg((const T2 *)P.tw4_hi + hi), __ldg((const T2 *)P.tw4_lo + lo));
 }
 
 // Epilogue for one complex output element kk of a transform whose column

@@ -340,6 +340,8 @@ const void *fftz_fast_f32_a(int log2n, int feat);
 const void *fftz_fast_f32_b(int log2n, int feat);
 const void *fftz_fast_f64_a(int log2n, int feat);
 const void *fftz_fast_f64_b(int log2n, int feat);
+const void *fftz_fast_f32_c(int log2n, int feat);
+const void *fftz_fast_f64_c(int log2n, int feat);
 
 static const void *fast_kernel(int dtype, int log2n, int variant) {
   int feat;
@@ -349,8 +351,11 @@ static const void *fast_kernel(int dtype, int log2n, int variant) {
     case FFTZ_VAR_FAST_TABS: feat = fftz::FEAT_TABS; break;
     case FFTZ_VAR_FAST_TW4_TABS: feat = fftz::FEAT_TW4 | fftz::FEAT_TABS; break;
     case FFTZ_VAR_FAST_BLUE: feat = fftz::FEAT_TABS | fftz::FEAT_SWEEP2; break;
+    case FFTZ_VAR_PIPE: feat = 16; break;
+    case FFTZ_VAR_PIPE_TW4: feat = 16 | fftz::FEAT_TW4; break;
     default: return 0;
   }
+  if (feat >= 16) return dtype == 0 ? fftz_fast_f32_c(log2n, feat) : fftz_fast_f64_c(log2n, feat);
   const void *f = dtype == 0 ? fftz_fast_f32_a(log2n, feat) : fftz_fast_f64_a(log2n, feat);
   if (!f) f = dtype == 0 ? fftz_fast_f32_b(log2n, feat) : fftz_fast_f64_b(log2n, feat);
   return f;
@@ -360,6 +365,7 @@ int fftz_max_smem_n(int dtype) { return dtype == 0 ? 16384 : 8192; }
 int fftz_fast_max_n(int dtype) { return dtype == 0 ? 16384 : 8192; }
 int fftz_fast_tpt(int n) { return fftz::ct_tpt(n); }
 int fftz_generic_max_threads(void) { return 256; }
+int fftz_pipe_max_threads(int n) { return fftz::ct_pipe_lb(n); }
 
 int fftz_fast_radices(int n, int32_t *radix) {
   const int S = fftz::ct_nstages(n);
@@ -375,6 +381,19 @@ int32_t fftz_smem_stride(int dtype, int32_t nslots) {
   while ((s & (m - 1)) != 1) s++;  // neighbouring transforms start on neighbouring banks
   return s;
 }
+
+int32_t fftz_smem_stride_cols(int dtype, int32_t nslots, int32_t tpc) {
+  const int sh = dtype == 0 ? (int)fftz::Cplx<float>::PADSH : (int)fftz::Cplx<double>::PADSH;
+  const int32_t w = 1 << sh;  // complex slots per 128-byte bank row
+  if (tpc <= 1 || tpc > w || (tpc & (tpc - 1))) return fftz_smem_stride(dtype, nslots);
+  if (nslots < 1) nslots = 1;
+  int32_t s = (nslots - 1) + ((nslots - 1) >> sh) + 1;
+  const int32_t want = w / tpc;  // transforms p and p+1 land w/tpc slots apart
+  while ((s & (w - 1)) != want) s++;
+  return s;
+}
+
+static int is_pipe(const fftz_pass_t *p) { return p->variant == FFTZ_VAR_PIPE || p->variant == FFTZ_VAR_PIPE_TW4; }
 
 int fftz_threads_per_transform(int dtype, int n, int nstages, const int32_t *radix) {
   (void)dtype;
@@ -394,6 +413,7 @@ int64_t fftz_smem_limit(void) { return 227 * 1024; }
 
 int64_t fftz_pass_smem_bytes(const fftz_pass_t *p) {
   const int64_t esz = p->dtype == 0 ? 8 : 16;
+  if (is_pipe(p)) return 2 * (int64_t)p->tpc * p->sstride * esz + 9 * 8 * (int64_t)p->tpc;
   return (int64_t)p->tpc * p->sstride * esz + 3 * 8 * (int64_t)p->tpc;
 }
 
@@ -423,8 +443,32 @@ int fftz_launch_pass(const fftz_pass_t *p, void *stream) {
     if (nopted[dev] < 96) opted[dev][nopted[dev]++] = fn;
   }
   const dim3 block((unsigned)(p->tpc * p->tpt));
-  const dim3 grid((unsigned)nblk);
   const size_t smem = (size_t)fftz_pass_smem_bytes(p);
+  dim3 grid((unsigned)nblk);
+  if (is_pipe(p)) {
+    // persistent: as many CTAs as fit on the device at once
+    static const void *occ_fn[64][32];
+    static size_t occ_smem[64][32];
+    static int occ_val[64][32], nocc[64], nsm[64];
+    int occ = 0;
+    for (int i = 0; i < nocc[dev]; i++)
+      if (occ_fn[dev][i] == fn && occ_smem[dev][i] == smem) occ = occ_val[dev][i];
+    if (!occ) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, (int)block.x, smem) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+      }
+      if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+      if (nocc[dev] < 32) {
+        occ_fn[dev][nocc[dev]] = fn;
+        occ_smem[dev][nocc[dev]] = smem;
+        occ_val[dev][nocc[dev]++] = occ;
+      }
+    }
+    if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+    const int64_t cap = (int64_t)occ * (nsm[dev] > 0 ? nsm[dev] : 148);
+    grid.x = (unsigned)(nblk < cap ? nblk : cap);
+  }
   void *args[1] = {(void *)p};
   return (int)cudaLaunchKernel(fn, grid, block, args, smem, (cudaStream_t)stream);
 }

@@ -49,6 +49,8 @@ enum fftz_out_kind {
 #define FFTZ_VAR_FAST_TABS 3 /* as FAST with load/store tables, bounds and scale     */
 #define FFTZ_VAR_FAST_TW4_TABS 4 /* both of the above                               */
 #define FFTZ_VAR_FAST_BLUE 5 /* tables plus two sweeps around a mid-table product   */
+#define FFTZ_VAR_PIPE 6      /* persistent, cp.async double-buffered, complex in/out */
+#define FFTZ_VAR_PIPE_TW4 7  /* as PIPE with the four-step twiddle epilogue         */
 
 /* pass flags */
 #define FFTZ_F_CONJ_IN    0x01 /* conjugate each loaded value (after kind decode) */
@@ -92,7 +94,7 @@ typedef struct fftz_pass
     const void *in;
     void *out;
     const void *tw;                     /* stage twiddles, working dtype */
-    const void *tw4_hi, *tw4_lo;        /* four-step twiddle factors, double2 */
+    const void *tw4_hi, *tw4_lo;        /* four-step twiddle factors, working dtype */
     const void *pre_tab, *post_tab, *mid_tab; /* working dtype complex */
     const void *rtw;                    /* packed-real twiddles W_{2M}^k, working dtype */
 } fftz_pass_t;
@@ -133,8 +135,9 @@ int fftz_fast_tpt(int n);
 int fftz_fast_max_n(int dtype);
 /* Radix list used by the compile-time kernel for length n (returns stages). */
 int fftz_fast_radices(int n, int32_t *radix);
-/* Threads per CTA the generic kernel may use. */
+/* Threads per CTA the generic kernel may use; the persistent kernels' bound. */
 int fftz_generic_max_threads(void);
+int fftz_pipe_max_threads(int n);
 
 /* Threads-per-transform needed so that no thread holds more than the
  * register budget in any stage (returns 0 if the plan is not executable). */
@@ -143,8 +146,11 @@ int fftz_threads_per_transform(int dtype, int n, int nstages, const int32_t *rad
 /* Shared memory bytes used by a pass with the given tpc/sstride. */
 int64_t fftz_pass_smem_bytes(const fftz_pass_t *p);
 
-/* Per-transform SMEM stride (complex slots) for nslots elements. */
+/* Per-transform SMEM stride (complex slots) for nslots elements; with tpc
+ * transforms per CTA mapped lane-wise (column maps) the stride also spreads
+ * the transforms over distinct banks. */
 int32_t fftz_smem_stride(int dtype, int32_t nslots);
+int32_t fftz_smem_stride_cols(int dtype, int32_t nslots, int32_t tpc);
 
 /* Maximum dynamic SMEM bytes per CTA the kernels may use. */
 int64_t fftz_smem_limit(void);

@@ -54,7 +54,8 @@ DescILP64 = _desc(Dim64)  # aoclfftz_prob_desc_f_64_ / _d_64_
 class Hints(C.Structure):
     """aoclfftz_gpu_hints_t (include/aoclfftz_gpu.h)."""
     _fields_ = [("fourstep_n1", C.c_int64), ("tpc_col", C.c_int32), ("tpc_row", C.c_int32),
-                ("batch_chunk", C.c_int64), ("algorithm", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("batch_chunk", C.c_int64), ("algorithm", C.c_int32), ("kernel_family", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 def bind(lib):

@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="fourstep24", choices=sorted(WORKLOADS))
+    ap.add_argument("--batch", type=int, default=0, help="override the workload's batch (small profiling cases)")
+    ap.add_argument("--fourstep-n1", type=int, default=0, help="planner hint: column length of the split")
+    ap.add_argument("--tpc-col", type=int, default=0, help="planner hint: transforms per CTA, column passes")
+    ap.add_argument("--family", type=int, default=0, help="planner hint: 1 one tile per CTA, 2 persistent")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -164,6 +168,9 @@ def run_ours(args, wl):
     dy = torch.empty_like(dx)
     dz = torch.empty_like(dx)
     stream = torch.cuda.Stream()
+    hints = abi.Hints()
+    hints.fourstep_n1, hints.tpc_col, hints.kernel_family = args.fourstep_n1, args.tpc_col, args.family
+    lib.aoclfftz_gpu_set_hints(C.byref(hints))
     pf = make_plan(lib, abi, dx.data_ptr(), dy.data_ptr(), n, b, 0, dtype)
     pb = make_plan(lib, abi, dy.data_ptr(), dz.data_ptr(), n, b, 1, dtype)
     for h in (pf, pb):
@@ -243,6 +250,7 @@ def run_ours(args, wl):
         hz = torch.empty_like(hx).pin_memory()
         qf = make_plan(lib, abi, hx.data_ptr(), hy.data_ptr(), n, b, 0, dtype)
         qb = make_plan(lib, abi, hy.data_ptr(), hz.data_ptr(), n, b, 1, dtype)
+        lib.aoclfftz_gpu_set_hints(None)
         for h in (qf, qb):
             lib.aoclfftz_gpu_set_stream(h, C.c_void_p(stream.cuda_stream))
 
@@ -273,6 +281,7 @@ def run_ours(args, wl):
                       "api": "aoclfftz_execute with pinned host in/out (library stages H2D, FFT, D2H)"}
         lib.aoclfftz_destroy(qf)
         lib.aoclfftz_destroy(qb)
+    lib.aoclfftz_gpu_set_hints(None)
     lib.aoclfftz_destroy(pf)
     lib.aoclfftz_destroy(pb)
     if ws > 1:
@@ -379,7 +388,10 @@ METRIC = "5N·log2N GFLOP/s + HBM GB/s vs plain GPU FFT at stated FP64 err, 1 B2
 
 def main():
     args = parse()
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.batch > 0:
+        wl["batch"] = args.batch
+        wl["desc"] = wl["desc"].replace("batch %d" % WORKLOADS[args.workload]["batch"], "batch %d" % args.batch)
     ws, rank, local = dist_env()
     if args.impl == "reference":
         out = run_reference(args, wl)

@@ -55,6 +55,7 @@ FFTZ_INT32 aoclfftz_gpu_pass_info(FFTZ_VOID *handle, FFTZ_INT32 i, FFTZ_CHAR *bu
  *   batch_chunk   multi-pass plans run their passes on chunks of this many
  *                 lines at a time (keeps the intermediate resident in L2)
  *   algorithm     1 one pass, 2 four-step, 3 Bluestein (0 = choose)
+ *   kernel_family 1 one tile per CTA, 2 persistent double-buffered (0 = choose)
  * aoclfftz_gpu_set_hints(NULL) restores the defaults. */
 typedef struct aoclfftz_gpu_hints
 {
@@ -63,7 +64,8 @@ typedef struct aoclfftz_gpu_hints
     FFTZ_INT32 tpc_row;
     FFTZ_INT64 batch_chunk;
     FFTZ_INT32 algorithm;
-    FFTZ_INT32 reserved[7];
+    FFTZ_INT32 kernel_family;
+    FFTZ_INT32 reserved[6];
 } aoclfftz_gpu_hints_t;
 
 aoclfftz_error_type aoclfftz_gpu_set_hints(const aoclfftz_gpu_hints_t *hints);

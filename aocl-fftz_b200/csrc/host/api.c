@@ -134,9 +134,10 @@ static int64_t span_elems(const fz_dim *dims, int rank, const fz_dim *vecs, int 
     return s;
 }
 
-static void plan_free(fz_plan *pl)
+void fz_plan_free(fz_plan *pl)
 {
     if (!pl) return;
+    if (pl->rg) fz_ragged_free(pl->rg);
     if (pl->dtab) cudaFree(pl->dtab);
     if (pl->scratch) cudaFree(pl->scratch);
     if (pl->stage) cudaFree(pl->stage);
@@ -177,7 +178,7 @@ static void *setup_impl(fz_desc *d, int dtype)
     if (cudaGetDevice(&pl->device) != cudaSuccess)
     {
         fz_set_error("no CUDA device available");
-        plan_free(pl);
+        fz_plan_free(pl);
         return NULL;
     }
     const int64_t esz = dtype == 0 ? 4 : 8;
@@ -200,7 +201,7 @@ static void *setup_impl(fz_desc *d, int dtype)
     if (fz_plan_build(pl, d->dim_rank, d->dims, d->vec_rank, d->vecs))
     {
         fz_log(pl, "setup failed: %s", g_err);
-        plan_free(pl);
+        fz_plan_free(pl);
         return NULL;
     }
     /* device tables: one allocation, then every pass's pointers */
@@ -211,7 +212,7 @@ static void *setup_impl(fz_desc *d, int dtype)
         {
             cudaGetLastError();
             fz_set_error("device allocation of %zu table bytes failed", pl->blob.len);
-            plan_free(pl);
+            fz_plan_free(pl);
             return NULL;
         }
     }
@@ -237,7 +238,7 @@ static void *setup_impl(fz_desc *d, int dtype)
     {
         cudaGetLastError();
         fz_set_error("device allocation of %lld scratch bytes failed", (long long)pl->scratch_bytes);
-        plan_free(pl);
+        fz_plan_free(pl);
         return NULL;
     }
     if (pl->log_mode >= AOCLFFTZ_LOG_INFO)
@@ -519,7 +520,7 @@ FFTZ_VOID aoclfftz_destroy(FFTZ_VOID *handle)
     if (!pl) return;
     if (pl->stream) cudaStreamSynchronize((cudaStream_t)pl->stream);
     else cudaDeviceSynchronize();
-    plan_free(pl);
+    fz_plan_free(pl);
 }
 
 const FFTZ_CHAR *aoclfftz_version(FFTZ_VOID) { return AOCLFFTZ_LIBRARY_VERSION " B200 (sm_100a)"; }
@@ -550,13 +551,24 @@ aoclfftz_error_type aoclfftz_gpu_synchronize(FFTZ_VOID *handle)
         fz_set_error("%s", cudaGetErrorString(e));
         return AOCLFFTZ_EXECUTION_FAILURE;
     }
+    if (pl->rg && pl->rg->d_err)
+    {
+        int flag = 0;
+        if (cudaMemcpy(&flag, pl->rg->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess || flag)
+        {
+            fz_set_error("ragged executor: a dependency wait gave up (results invalid)");
+            return AOCLFFTZ_EXECUTION_FAILURE;
+        }
+    }
     return AOCLFFTZ_SUCCESS;
 }
 
 FFTZ_INT32 aoclfftz_gpu_num_launches(FFTZ_VOID *handle)
 {
     fz_plan *pl = as_plan(handle);
-    return pl ? (pl->nop ? 0 : pl->nlaunch) : -1;
+    if (!pl) return -1;
+    if (pl->rg) return 1;
+    return pl->nop ? 0 : pl->nlaunch;
 }
 
 FFTZ_INT32 aoclfftz_gpu_describe(FFTZ_VOID *handle, FFTZ_CHAR *buf, FFTZ_INT32 len)
@@ -566,6 +578,7 @@ FFTZ_INT32 aoclfftz_gpu_describe(FFTZ_VOID *handle, FFTZ_CHAR *buf, FFTZ_INT32 l
     int w = snprintf(buf, (size_t)len, "%s %s %s %s:", pl->dtype ? "f64" : "f32", pl->fft_type ? "real" : "c2c",
                      pl->direction ? "bwd" : "fwd", pl->placement ? "oop" : "inplace");
     if (pl->nop && w < len) w += snprintf(buf + w, (size_t)(len - w), " empty batch");
+    if (pl->rg && w < len) w += snprintf(buf + w, (size_t)(len - w), " %s", pl->rg->summary);
     for (int i = 0; i < pl->npass && w < len; i++)
         w += pl->pass[i].is_elem ? snprintf(buf + w, (size_t)(len - w), " [%s]", pl->pass[i].what)
                                   : snprintf(buf + w, (size_t)(len - w), " [%s tpc=%d tpt=%d]", pl->pass[i].what,

@@ -53,6 +53,20 @@ typedef struct
     size_t len, cap;
 } fz_blob;
 
+/* ragged batch state (ragged.c): one persistent launch over all tiles */
+typedef struct fz_ragged
+{
+    int64_t count, npasses, nitems;
+    int64_t in_elems, out_elems; /* complex elements the buffers span */
+    void *d_passes, *d_items, *d_done, *d_queue, *d_err;
+    int grid, smem;
+    void *cap_stream;             /* stream used to capture the graph */
+    void *graph, *graph_exec;     /* cudaGraph_t / cudaGraphExec_t */
+    const void *g_in;             /* buffers the graph was captured with */
+    void *g_out;
+    char summary[160];
+} fz_ragged;
+
 typedef struct fz_plan
 {
     uint32_t magic;
@@ -81,6 +95,7 @@ typedef struct fz_plan
     int scratch_busy; /* 1 while an execute holds the plan's scratch */
     int nlaunch;
     aoclfftz_gpu_hints_t hints;
+    fz_ragged *rg; /* non-NULL for ragged-batch handles */
     /* per-pass event timing: prof_cap executes x npass x {start, end} */
     void **prof_ev;
     int prof_cap, prof_n;
@@ -102,6 +117,10 @@ int fz_bluestein_tables(fz_blob *b, int dtype, int64_t n, int64_t m, int directi
                         int64_t *off_post, int64_t *off_mid);
 /* packed-real twiddles W_{2M}^k, k = 0..M (W^M = -1) */
 int64_t fz_real_twiddles(fz_blob *b, int dtype, int64_t M);
+
+/* ---- shared by api.c and ragged.c ---- */
+void fz_plan_free(fz_plan *pl);
+void fz_ragged_free(fz_ragged *rg);
 
 /* ---- planner (plan.c) ---- */
 int fz_plan_build(fz_plan *pl, int rank, const fz_dim *dims, int vrank, const fz_dim *vecs);

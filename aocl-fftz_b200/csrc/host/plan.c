@@ -96,6 +96,9 @@ static fz_pass *push_pass(fz_plan *pl)
 
 static int64_t absl(int64_t x) { return x < 0 ? -x : x; }
 
+/* every pass on the generic kernel (the persistent executor runs only that) */
+static int generic_only(const fz_plan *pl) { return pl->hints.kernel_family == 3; }
+
 /* Batch dims: optionally sorted by stride (smallest first, so that bdim[0]
  * is the one lanes may run along), then adjacent dims merged when they form
  * one arithmetic progression on both sides (the reference's fuse_vecs,
@@ -211,7 +214,7 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
     p->dst = dst;
     if (set_batch(k, b, nb, keep_first)) return NULL;
     set_modes(k);
-    const int fast = is_pow2(n) && n >= 2 && n <= fftz_fast_max_n(pl->dtype);
+    const int fast = !generic_only(pl) && is_pow2(n) && n >= 2 && n <= fftz_fast_max_n(pl->dtype);
     int maxthr;
     if (fast)
     {
@@ -296,7 +299,7 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
 static int single_pass_ok(const fz_plan *pl, int64_t n)
 {
     if (n == 1) return 1;
-    if (is_pow2(n) && n <= fftz_fast_max_n(pl->dtype)) return 1;
+    if (!generic_only(pl) && is_pow2(n) && n <= fftz_fast_max_n(pl->dtype)) return 1;
     int32_t r[FFTZ_MAX_STAGES];
     int s = generic_radices(n, r);
     if (s < 0) return 0;
@@ -474,7 +477,7 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
     int64_t pre, post, mid;
     if (fz_bluestein_tables(&pl->blob, pl->dtype, n, m, pl->direction, &pre, &post, &mid)) return -1;
     const int bwd = pl->direction == 1;
-    if (m <= fftz_fast_max_n(pl->dtype) && m >= 4)
+    if (m >= 4 && single_pass_ok(pl, m))
     {
         fz_pass *p = line_pass(pl, m, ies, oes, b, nb, 0, src, dst,
                                (bwd ? FFTZ_F_CONJ_IN : FFTZ_F_CONJ_OUT) | FFTZ_F_PRE_TAB | FFTZ_F_POST_TAB |

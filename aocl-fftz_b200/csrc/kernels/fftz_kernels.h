@@ -97,7 +97,44 @@ typedef struct fftz_pass
     const void *tw4_hi, *tw4_lo;        /* four-step twiddle factors, working dtype */
     const void *pre_tab, *post_tab, *mid_tab; /* working dtype complex */
     const void *rtw;                    /* packed-real twiddles W_{2M}^k, working dtype */
+    /* persistent executor only: in / out hold byte offsets into these bases */
+    int32_t src_buf, dst_buf;           /* FFTZ_RBUF_* */
 } fftz_pass_t;
+
+/* Persistent DAG executor (fft_ragged.cu): one launch runs the CTA tiles of
+ * many passes; a tile of a pass with a predecessor waits until every tile of
+ * the predecessor has completed. */
+#define FFTZ_RBUF_IN 0
+#define FFTZ_RBUF_OUT 1
+#define FFTZ_RBUF_SCRATCH 2
+
+typedef struct fftz_ritem
+{
+    int32_t pass;      /* index into the pass table */
+    int32_t dep;       /* pass that must complete first, -1 if none */
+    int64_t blk;       /* CTA tile of the pass */
+    int64_t dep_count; /* tiles of dep */
+} fftz_ritem_t;
+
+typedef struct fftz_ragged
+{
+    const fftz_pass_t *passes;
+    const fftz_ritem_t *items;
+    int64_t nitems;
+    unsigned long long *queue; /* next item to take */
+    int *done;                 /* completed tiles per pass */
+    int *err;                  /* set when a wait gave up */
+    const void *in;
+    void *out;
+    void *scratch;
+    int64_t spin_limit;        /* polls before a wait gives up */
+    int32_t dtype;
+    int32_t smem_bytes;
+} fftz_ragged_t;
+
+int fftz_launch_ragged(const fftz_ragged_t *r, int grid, void *stream);
+/* CTAs of the persistent executor that fit on the device at once. */
+int fftz_ragged_grid(int dtype, int smem_bytes);
 
 /* Elementwise real-transform helpers (fft_elem.cu) */
 enum fftz_elem_mode {

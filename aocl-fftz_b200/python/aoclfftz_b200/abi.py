@@ -100,6 +100,11 @@ def bind_gpu(lib):
     lib.aoclfftz_gpu_pass_info.restype = C.c_int32
     lib.aoclfftz_gpu_set_hints.argtypes = [C.c_void_p]
     lib.aoclfftz_gpu_set_hints.restype = C.c_int
+    lib.aoclfftz_gpu_ragged_setup.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.POINTER(C.c_int64),
+                                              C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.aoclfftz_gpu_ragged_setup.restype = C.c_void_p
+    lib.aoclfftz_gpu_ragged_execute.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.aoclfftz_gpu_ragged_execute.restype = C.c_int
     lib.aoclfftz_gpu_last_error.argtypes = []
     lib.aoclfftz_gpu_last_error.restype = C.c_char_p
     return lib

@@ -51,3 +51,59 @@ def complex_uniform(seed, n, dtype=np.complex64):
 def complex_normal(seed, n, dtype=np.complex128):
     v = normal(seed, 2 * n)
     return (v[0::2] + 1j * v[1::2]).astype(dtype)
+
+
+def _next_pow2(n):
+    p = 1
+    while p < n:
+        p *= 2
+    return p
+
+
+def _smooth7(n):
+    for p in (2, 3, 5, 7):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
+def _is_prime(n):
+    if n < 2:
+        return False
+    if n % 2 == 0:
+        return n == 2
+    f = 3
+    while f * f <= n:
+        if n % f == 0:
+            return False
+        f += 2
+    return True
+
+
+def ragged_sizes(seed, count, lo=2, hi=65536):
+    """Transform lengths of a ragged batch: N0 = round(exp(u)), u ~ U[ln lo, ln hi],
+    then one third each (by a second draw) rounded up to the next power of two,
+    the next 7-smooth number, or the next prime, clamped to hi."""
+    u = u01(seed, 2 * count)
+    out = []
+    for i in range(count):
+        n0 = int(round(np.exp(np.log(lo) + u[2 * i] * (np.log(hi) - np.log(lo)))))
+        n0 = max(lo, min(hi, n0))
+        cls = int(u[2 * i + 1] * 3)
+        if cls == 0:
+            n = _next_pow2(n0)
+        elif cls == 1:
+            n = n0
+            while not _smooth7(n):
+                n += 1
+        else:
+            n = n0
+            while not _is_prime(n):
+                n += 1
+        if n > hi:
+            n = hi
+            if cls == 2:
+                while not _is_prime(n):
+                    n -= 1
+        out.append(n)
+    return out

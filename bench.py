@@ -36,6 +36,13 @@ WORKLOADS = {
                        desc="c2c fp32 N=2^24 (4096x4096 four-step) batch 4, out-of-place, fwd+bwd"),
     "batch4096": dict(n=4096, batch=1024, dtype="f32",
                       desc="c2c fp32 N=4096 batch 1024, out-of-place, fwd+bwd"),
+    "ragged": dict(n=0, batch=4096, dtype="f32", ragged=True,
+                   desc="ragged batch of 4096 c2c fp32 transforms, lengths log-uniform in [2, 65536] "
+                        "(pow2 / 7-smooth / prime thirds), packed, one persistent launch under a CUDA graph, fwd+bwd"),
+    "ragged_f64": dict(n=0, batch=4096, dtype="f64", ragged=True,
+                       desc="ragged batch of 4096 c2c fp64 transforms, lengths log-uniform in [2, 65536] "
+                            "(pow2 / 7-smooth / prime thirds), packed, one persistent launch under a CUDA graph, "
+                            "fwd+bwd"),
 }
 
 
@@ -290,6 +297,114 @@ def run_ours(args, wl):
     return res
 
 
+def run_ragged(args, wl):
+    """Ragged batch: one graph launch per direction (aoclfftz_gpu_ragged_*)
+    against the plain path (one aoclfftz plan per transform, executed back to
+    back on the same stream)."""
+    import numpy as np
+    import torch
+
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi, synthetic
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = aoclfftz_b200.load()
+    dtype = wl["dtype"]
+    dt = 0 if dtype == "f32" else 1
+    esz = 8 if dtype == "f32" else 16
+    sizes = synthetic.ragged_sizes(4242, wl["batch"], 2, 65536)
+    total = int(sum(sizes))
+    cd = np.complex64 if dtype == "f32" else np.complex128
+    x = synthetic.complex_normal(4243, total, cd)
+    dx = torch.from_numpy(x.view(x.real.dtype).copy()).to("cuda")
+    dy = torch.empty_like(dx)
+    dz = torch.empty_like(dx)
+    stream = torch.cuda.Stream()
+    arr = (C.c_int64 * len(sizes))(*sizes)
+    t0 = time.perf_counter()
+    hf = lib.aoclfftz_gpu_ragged_setup(dt, 0, len(sizes), arr, None, None)
+    hb = lib.aoclfftz_gpu_ragged_setup(dt, 1, len(sizes), arr, None, None)
+    setup_s = time.perf_counter() - t0
+    if not hf or not hb:
+        raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
+    for h in (hf, hb):
+        lib.aoclfftz_gpu_set_stream(h, C.c_void_p(stream.cuda_stream))
+    pin, py, pz = C.c_void_p(dx.data_ptr()), C.c_void_p(dy.data_ptr()), C.c_void_p(dz.data_ptr())
+
+    def step():
+        if lib.aoclfftz_gpu_ragged_execute(hf, pin, py) or lib.aoclfftz_gpu_ragged_execute(hb, py, pz):
+            raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    if lib.aoclfftz_gpu_synchronize(hf) or lib.aoclfftz_gpu_synchronize(hb):
+        raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
+    zc = dz.view(torch.complex64 if dtype == "f32" else torch.complex128).cpu().numpy()
+    offs = np.cumsum([0] + sizes[:-1])
+    rt = max(float(np.linalg.norm(zc[o:o + n] / n - x[o:o + n]) / max(np.linalg.norm(x[o:o + n]), 1e-30))
+             for o, n in zip(offs, sizes))
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ms = timed(step, args.steps)
+    clk = clocks.stop()
+    # plain path: one ordinary plan per transform, same stream
+    plans = []
+    t0 = time.perf_counter()
+    for d, a, b in ((0, dx, dy), (1, dy, dz)):
+        for o, n in zip(offs, sizes):
+            desc, keep = abi.make_desc(a.data_ptr() + int(o) * esz, b.data_ptr() + int(o) * esz, [(n, 1, 1)],
+                                       [(1, n, n)], 0, d, 1)
+            h = abi.setup(lib, desc, dtype)
+            if not h:
+                raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
+            lib.aoclfftz_gpu_set_stream(h, C.c_void_p(stream.cuda_stream))
+            plans.append(h)
+    plain_setup_s = time.perf_counter() - t0
+    launches_plain = sum(lib.aoclfftz_gpu_num_launches(h) for h in plans)
+
+    def plain_step():
+        for h in plans:
+            lib.aoclfftz_execute(h)
+
+    plain_step()
+    ms_plain = timed(plain_step, max(2, min(args.steps, 5)))
+    for h in plans:
+        lib.aoclfftz_destroy(h)
+    flops = 2 * sum(5.0 * n * math.log2(n) for n in sizes if n > 1)
+    alg_bytes = 2 * 2 * total * esz
+    txt = C.create_string_buffer(512)
+    lib.aoclfftz_gpu_describe(hf, txt, 512)
+    lib.aoclfftz_destroy(hf)
+    lib.aoclfftz_destroy(hb)
+    peak, peak_kind = load_peaks()
+    per_launch = total * 2 * esz  # one read + one write of the packed batch
+    achieved = per_launch / (ms / 2 * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None, "kernel": "fft_ragged_kernel (one launch per direction)",
+            "bytes_per_launch": per_launch, "ms_per_launch": round(ms / 2, 5),
+            "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind}
+    return dict(ms=ms, value=flops / (ms * 1e-3) / 1e9, hbm_gbs=alg_bytes / (ms * 1e-3) / 1e9, rt_err=rt,
+                clocks=clk, launches=2 * args.steps, roofline=roof,
+                extra={"plain_path": {"ms_per_step": round(ms_plain, 4),
+                                      "value": round(flops / (ms_plain * 1e-3) / 1e9, 2),
+                                      "launches_per_step": launches_plain, "setup_s": round(plain_setup_s, 2)},
+                       "speedup_vs_plain": round(ms_plain / ms, 2), "ragged_setup_s": round(setup_s, 2),
+                       "plan": txt.value.decode(), "total_elements": total,
+                       "sizes": {"count": len(sizes), "min": min(sizes), "max": max(sizes)}})
+
+
 def time_reference(wl, threads, transforms, steps, warmup, min_time=None):
     """The reference library's own CPU path (AOCL-FFTZ compiled from its
     sources into oracle/_ref/, OpenMP) through aoclfftz_setup_f/execute on host
@@ -398,7 +513,7 @@ def main():
         if out is not None:
             print(json.dumps(out))
         return
-    r = run_ours(args, wl)
+    r = run_ragged(args, wl) if wl.get("ragged") else run_ours(args, wl)
     if rank != 0:
         return
     peak, peak_kind = load_peaks()
@@ -410,11 +525,14 @@ def main():
                        if wl["n"] * wl["batch"] * 8 > 126e6 else "inputs fit L2",
                        "parallelism": "replicas dp%d" % ws},
             "hbm_gbs": round(r["hbm_gbs"], 1), "hbm_frac_of_measured": round(r["hbm_gbs"] / peak, 4),
-            "roofline": r["roofline"], "gpu_launches": r["launches"], "clocks": r["clocks"],
-            "round_trip_rel_l2": r["rt_err"], "passes": r["passes"]}
+            "gpu_launches": r["launches"], "clocks": r["clocks"], "round_trip_rel_l2": r["rt_err"]}
+    for key in ("roofline", "passes"):
+        if key in r:
+            line[key] = r[key]
+    line.update(r.get("extra", {}))
     if "e2e" in r:
         line["e2e"] = r["e2e"]
-    if ws == 1 and not args.no_cpu_baseline:
+    if ws == 1 and not args.no_cpu_baseline and not wl.get("ragged"):
         try:
             line["cpu_baseline"] = cpu_baseline(wl)
         except Exception as e:  # the baseline is reported, never required

@@ -70,6 +70,20 @@ typedef struct aoclfftz_gpu_hints
 
 aoclfftz_error_type aoclfftz_gpu_set_hints(const aoclfftz_gpu_hints_t *hints);
 
+/* Ragged batches: `count` independent 1-D c2c transforms of different lengths
+ * (any length: powers of two, smooth composites, primes via Bluestein) in one
+ * persistent kernel launch, captured once in a CUDA graph. dtype 0 = float,
+ * 1 = double; direction 0 = forward, 1 = backward. Transform i reads sizes[i]
+ * contiguous complex elements at in + in_offsets[i] and writes out +
+ * out_offsets[i] (offsets in complex elements; NULL = packed back to back).
+ * Execute takes device buffers (out of place); the handle is released with
+ * aoclfftz_destroy and works with aoclfftz_gpu_set_stream / _synchronize
+ * (which also reports a failed dependency wait). */
+FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFTZ_INT64 count,
+                                     const FFTZ_INT64 *sizes, const FFTZ_INT64 *in_offsets,
+                                     const FFTZ_INT64 *out_offsets);
+aoclfftz_error_type aoclfftz_gpu_ragged_execute(FFTZ_VOID *handle, FFTZ_VOID *in, FFTZ_VOID *out);
+
 /* Text of the last error recorded by this thread (empty if none). */
 const FFTZ_CHAR *aoclfftz_gpu_last_error(FFTZ_VOID);
 

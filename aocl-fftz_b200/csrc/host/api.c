@@ -147,6 +147,10 @@ void fz_plan_free(fz_plan *pl)
             if (pl->prof_ev[i]) cudaEventDestroy((cudaEvent_t)pl->prof_ev[i]);
         free(pl->prof_ev);
     }
+    if (pl->chunk) fz_plan_free(pl->chunk);
+    for (int i = 0; i < 3; i++)
+        if (pl->pipe_stream[i]) cudaStreamDestroy((cudaStream_t)pl->pipe_stream[i]);
+    if (pl->pipe_buf) cudaFree(pl->pipe_buf);
     free(pl->pass);
     free(pl->blob.p);
     pl->magic = 0;
@@ -198,6 +202,10 @@ static void *setup_impl(fz_desc *d, int dtype)
         pl->in_bytes = span_elems(d->dims, d->dim_rank, d->vecs, d->vec_rank, 0, n0 / 2 + 1) * 2 * esz;
         pl->out_bytes = span_elems(d->dims, d->dim_rank, d->vecs, d->vec_rank, 1, 0) * esz;
     }
+    pl->sv_rank = d->dim_rank;
+    pl->sv_vrank = d->vec_rank;
+    memcpy(pl->sv_dims, d->dims, sizeof(fz_dim) * (size_t)d->dim_rank);
+    memcpy(pl->sv_vecs, d->vecs, sizeof(fz_dim) * (size_t)d->vec_rank);
     if (fz_plan_build(pl, d->dim_rank, d->dims, d->vec_rank, d->vecs))
     {
         fz_log(pl, "setup failed: %s", g_err);
@@ -358,6 +366,165 @@ static int device_usable(const void *p)
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+static void *setup_impl(fz_desc *d, int dtype);
+
+static int is_pinned(const void *p)
+{
+    struct cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+/* Builds the chunk plan: the same descriptor with the outermost batch
+ * dimension cut to chunk_c entries (a divisor of its length), so that
+ * consecutive chunks are contiguous byte ranges on both sides. */
+static int prepare_chunks(fz_plan *pl)
+{
+    pl->chunk_state = -1;
+    if (pl->sv_vrank < 1 || pl->nop) return -1;
+    int o = 0;
+    for (int i = 1; i < pl->sv_vrank; i++)
+        if (pl->sv_vecs[i].is > pl->sv_vecs[o].is) o = i;
+    const fz_dim outer = pl->sv_vecs[o];
+    if (outer.n < 2) return -1;
+    for (int i = 0; i < pl->sv_rank; i++)
+        if (pl->sv_dims[i].is * pl->sv_dims[i].n > outer.is || pl->sv_dims[i].os * pl->sv_dims[i].n > outer.os)
+            return -1;
+    for (int i = 0; i < pl->sv_vrank; i++)
+        if (i != o && (pl->sv_vecs[i].is * pl->sv_vecs[i].n > outer.is || pl->sv_vecs[i].os * pl->sv_vecs[i].n > outer.os))
+            return -1;
+    /* about 8 chunks of at least 4 MiB each */
+    const int64_t per_entry = pl->in_bytes / outer.n + 1;
+    int64_t target = outer.n / 8;
+    if (target < 1) target = 1;
+    while (target > 1 && target * per_entry < (4 << 20) && target * 2 <= outer.n / 2) target *= 2;
+    int64_t c = target;
+    while (c > 1 && outer.n % c) c--;
+    if (outer.n / c < 2) return -1;
+    fz_desc d;
+    memset(&d, 0, sizeof(d));
+    aoclfftz_flags_t f;
+    memset(&f, 0, sizeof(f));
+    f.fft_type = (FFTZ_UINT8)pl->fft_type;
+    f.fft_direction = (FFTZ_UINT8)pl->direction;
+    f.fft_placement = (FFTZ_UINT8)pl->placement;
+    aoclfftz_cntrl_params_t cp;
+    memset(&cp, 0, sizeof(cp));
+    cp.opt_level = 3;
+    aoclfftz_smp_pfft_t pt = {1, 1};
+    d.flags = &f;
+    d.cp = &cp;
+    d.pt = &pt;
+    d.dim_rank = pl->sv_rank;
+    d.vec_rank = pl->sv_vrank;
+    memcpy(d.dims, pl->sv_dims, sizeof(fz_dim) * (size_t)pl->sv_rank);
+    memcpy(d.vecs, pl->sv_vecs, sizeof(fz_dim) * (size_t)pl->sv_vrank);
+    d.vecs[o].n = c;
+    /* placeholder device-side addresses with the right placement */
+    d.in = (void *)(uintptr_t)0x1000;
+    d.out = pl->placement == 0 ? d.in : (void *)(uintptr_t)0x2000;
+    aoclfftz_gpu_hints_t saved = g_hints;
+    g_hints = pl->hints;
+    fz_plan *ch = (fz_plan *)setup_impl(&d, pl->dtype);
+    g_hints = saved;
+    if (!ch) return -1;
+    ch->stream = NULL;
+    const int64_t esz_in = (pl->fft_type == 0 || pl->direction == 1) ? (pl->dtype == 0 ? 8 : 16) : (pl->dtype == 0 ? 4 : 8);
+    const int64_t esz_out = (pl->fft_type == 0 || pl->direction == 0) ? (pl->dtype == 0 ? 8 : 16) : (pl->dtype == 0 ? 4 : 8);
+    pl->chunk = ch;
+    pl->chunk_c = c;
+    pl->chunk_count = outer.n / c;
+    pl->chunk_in_step = c * outer.is * esz_in;
+    pl->chunk_out_step = c * outer.os * esz_out;
+    pl->pipe_in_bytes = (ch->in_bytes + 255) & ~(int64_t)255;
+    pl->pipe_out_bytes = pl->placement == 0 ? 0 : (ch->out_bytes + 255) & ~(int64_t)255;
+    if (pl->placement == 0 && ch->out_bytes > ch->in_bytes) pl->pipe_in_bytes = (ch->out_bytes + 255) & ~(int64_t)255;
+    pl->pipe_slot_bytes = pl->pipe_in_bytes + pl->pipe_out_bytes + ((ch->scratch_bytes + 255) & ~(int64_t)255);
+    if (cudaMalloc(&pl->pipe_buf, (size_t)(3 * pl->pipe_slot_bytes)) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return -1;
+    }
+    for (int i = 0; i < 3; i++)
+        if (cudaStreamCreateWithFlags((cudaStream_t *)&pl->pipe_stream[i], cudaStreamNonBlocking) != cudaSuccess)
+            return -1;
+    pl->chunk_state = 1;
+    return 0;
+}
+
+/* Launches the passes of plan `ch` with the given buffer bases on stream st. */
+static int launch_passes(fz_plan *ch, void *in, void *out, void *scratch, cudaStream_t st)
+{
+    void *buf[FZ_NBUF];
+    buf[FZ_BUF_IN] = in;
+    buf[FZ_BUF_OUT] = out;
+    int64_t off = 0;
+    for (int i = 0; i < ch->nscratch; i++)
+    {
+        buf[FZ_BUF_SCR0 + i] = (unsigned char *)scratch + off;
+        off += (ch->scratch_elems[i] * 2 * (ch->dtype == 0 ? 4 : 8) + 255) & ~(int64_t)255;
+    }
+    for (int i = 0; i < ch->npass; i++)
+    {
+        int e;
+        if (ch->pass[i].is_elem)
+        {
+            fftz_elem_t el = ch->pass[i].e;
+            el.in = (const unsigned char *)buf[ch->pass[i].src] + ch->pass[i].in_off;
+            el.out = (unsigned char *)buf[ch->pass[i].dst] + ch->pass[i].out_off;
+            e = fftz_launch_elem(&el, st);
+        }
+        else
+        {
+            fftz_pass_t k = ch->pass[i].k;
+            k.in = (const unsigned char *)buf[ch->pass[i].src] + ch->pass[i].in_off;
+            k.out = (unsigned char *)buf[ch->pass[i].dst] + ch->pass[i].out_off;
+            e = fftz_launch_pass(&k, st);
+        }
+        if (e) return e;
+    }
+    return 0;
+}
+
+/* Host buffers in page-locked memory: chunk i is copied in on slot i % 3's
+ * stream, transformed, and copied out, so copy-in of one chunk, the passes
+ * of the next and copy-out of the previous overlap. */
+static aoclfftz_error_type run_pipelined(fz_plan *pl, void *in, void *out)
+{
+    cudaStream_t ps = (cudaStream_t)pl->stream;
+    cudaEvent_t ready;
+    if (cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess) return AOCLFFTZ_EXECUTION_FAILURE;
+    cudaEventRecord(ready, ps); /* work already queued on the plan's stream comes first */
+    int err = 0;
+    for (int i = 0; i < 3; i++) cudaStreamWaitEvent((cudaStream_t)pl->pipe_stream[i], ready, 0);
+    for (int64_t c = 0; c < pl->chunk_count && !err; c++)
+    {
+        const int slot = (int)(c % 3);
+        cudaStream_t st = (cudaStream_t)pl->pipe_stream[slot];
+        unsigned char *sb = (unsigned char *)pl->pipe_buf + slot * pl->pipe_slot_bytes;
+        unsigned char *din = sb, *dout = pl->placement == 0 ? sb : sb + pl->pipe_in_bytes;
+        unsigned char *scr = sb + pl->pipe_in_bytes + pl->pipe_out_bytes;
+        err |= cudaMemcpyAsync(din, (unsigned char *)in + c * pl->chunk_in_step, (size_t)pl->chunk->in_bytes,
+                               cudaMemcpyHostToDevice, st) != cudaSuccess;
+        err |= launch_passes(pl->chunk, din, dout, scr, st) != 0;
+        err |= cudaMemcpyAsync((unsigned char *)out + c * pl->chunk_out_step, dout, (size_t)pl->chunk->out_bytes,
+                               cudaMemcpyDeviceToHost, st) != cudaSuccess;
+    }
+    for (int i = 0; i < 3; i++)
+        if (cudaStreamSynchronize((cudaStream_t)pl->pipe_stream[i]) != cudaSuccess) err = 1;
+    cudaEventDestroy(ready);
+    if (err)
+    {
+        fz_set_error("pipelined host execution failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return AOCLFFTZ_EXECUTION_FAILURE;
+    }
+    return AOCLFFTZ_SUCCESS;
+}
+
 static aoclfftz_error_type run(fz_plan *pl, void *in, void *out)
 {
     if (pl->nop) return AOCLFFTZ_SUCCESS;
@@ -368,6 +535,20 @@ static aoclfftz_error_type run(fz_plan *pl, void *in, void *out)
     const int in_dev = device_usable(in);
     const int out_dev = device_usable(out);
     const int inplace = (in == out);
+    if (!in_dev && !out_dev && !pl->prof_ev && is_pinned(in) && is_pinned(out))
+    {
+        /* one pipelined execute at a time per plan (the staging slots are shared) */
+        int expect = 0;
+        if (__atomic_compare_exchange_n(&pl->scratch_busy, &expect, 1, 0, __ATOMIC_ACQ_REL, __ATOMIC_ACQUIRE))
+        {
+            if (pl->chunk_state == 0) prepare_chunks(pl);
+            aoclfftz_error_type r = AOCLFFTZ_SUCCESS;
+            int used = pl->chunk_state == 1;
+            if (used) r = run_pipelined(pl, in, out);
+            __atomic_store_n(&pl->scratch_busy, 0, __ATOMIC_RELEASE);
+            if (used) return r;
+        }
+    }
     /* ownership of the plan's scratch and staging memory */
     int expected = 0;
     const int owner = __atomic_compare_exchange_n(&pl->scratch_busy, &expected, 1, 0, __ATOMIC_ACQ_REL,

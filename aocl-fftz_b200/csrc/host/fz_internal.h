@@ -96,6 +96,17 @@ typedef struct fz_plan
     int nlaunch;
     aoclfftz_gpu_hints_t hints;
     fz_ragged *rg; /* non-NULL for ragged-batch handles */
+    /* the descriptor (for the chunk plan of pipelined host staging) */
+    fz_dim sv_dims[16], sv_vecs[16];
+    int sv_rank, sv_vrank;
+    /* pipelined host staging: chunks of the outermost batch dimension run
+     * copy-in / passes / copy-out on FZ_PIPE_SLOTS streams */
+    struct fz_plan *chunk;   /* plan of one chunk (built at the first pinned-host execute) */
+    int64_t chunk_c, chunk_count, chunk_in_step, chunk_out_step; /* entries, chunks, bytes */
+    int chunk_state;         /* 0 not tried, 1 ready, -1 not chunkable */
+    void *pipe_stream[3];
+    void *pipe_buf;          /* per slot: staging in, staging out, scratch */
+    int64_t pipe_slot_bytes, pipe_in_bytes, pipe_out_bytes;
     /* per-pass event timing: prof_cap executes x npass x {start, end} */
     void **prof_ev;
     int prof_cap, prof_n;

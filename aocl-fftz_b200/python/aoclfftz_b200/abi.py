@@ -105,6 +105,15 @@ def bind_gpu(lib):
     lib.aoclfftz_gpu_ragged_setup.restype = C.c_void_p
     lib.aoclfftz_gpu_ragged_execute.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.aoclfftz_gpu_ragged_execute.restype = C.c_int
+    fp = C.c_void_p
+    lib.aoclfftz_gpu_mlp_nparams.argtypes = [C.c_int32]
+    lib.aoclfftz_gpu_mlp_nparams.restype = C.c_int32
+    lib.aoclfftz_gpu_mlp_forward.argtypes = [fp, C.c_int32, fp, C.c_int32, fp, fp, fp]
+    lib.aoclfftz_gpu_mlp_forward.restype = C.c_int32
+    lib.aoclfftz_gpu_mlp_grad.argtypes = [fp, C.c_int32, fp, fp, C.c_int32, fp, fp, fp, fp]
+    lib.aoclfftz_gpu_mlp_grad.restype = C.c_int32
+    lib.aoclfftz_gpu_mlp_adam.argtypes = [fp, fp, fp, fp, C.c_int32, C.c_float, C.c_int32, fp]
+    lib.aoclfftz_gpu_mlp_adam.restype = C.c_int32
     lib.aoclfftz_gpu_last_error.argtypes = []
     lib.aoclfftz_gpu_last_error.restype = C.c_char_p
     return lib

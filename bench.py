@@ -39,6 +39,10 @@ WORKLOADS = {
     "ragged": dict(n=0, batch=4096, dtype="f32", ragged=True,
                    desc="ragged batch of 4096 c2c fp32 transforms, lengths log-uniform in [2, 65536] "
                         "(pow2 / 7-smooth / prime thirds), packed, one persistent launch under a CUDA graph, fwd+bwd"),
+    "selector": dict(n=0, batch=2500, dtype="mixed", selector=True,
+                     desc="learned plan selector: seeded problems (rank 1-3, pow2 / 7-smooth / prime dims, "
+                          "c2c/r2c/c2r, f32/f64, unit or strided, batch 1-256, <= 2^22 elements); candidates "
+                          "timed by the autotuner; 2x64 MLP trained on 80% of problems, regret on the rest"),
     "ragged_f64": dict(n=0, batch=4096, dtype="f64", ragged=True,
                        desc="ragged batch of 4096 c2c fp64 transforms, lengths log-uniform in [2, 65536] "
                             "(pow2 / 7-smooth / prime thirds), packed, one persistent launch under a CUDA graph, "
@@ -405,6 +409,55 @@ def run_ragged(args, wl):
                        "sizes": {"count": len(sizes), "min": min(sizes), "max": max(sizes)}})
 
 
+def run_selector(args, wl):
+    """Autotuner timings -> MLP trained on the GPU -> held-out regret against
+    exhaustive search, next to the planner's default choice."""
+    import numpy as np
+    import torch
+
+    import aoclfftz_b200
+    from aoclfftz_b200 import selector
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = aoclfftz_b200.load()
+    nprob = wl["batch"]
+    probs = selector.random_problems(20261203, nprob)
+    t0 = time.perf_counter()
+    data = []
+    for p in probs:
+        c = selector.time_candidates(lib, p)
+        if len(c) >= 1:
+            data.append((p, c))
+    tune_s = time.perf_counter() - t0
+    ntrain = int(0.8 * len(data))
+    train, test = data[:ntrain], data[ntrain:]
+    X = np.stack([f for _, cs in train for (_, _, f, _) in cs])
+    y = np.log(np.array([ms for _, cs in train for (_, _, _, ms) in cs]) * 1e3)  # log microseconds
+    sel = selector.MLPSelector(lib)
+    t1 = time.perf_counter()
+    hist = sel.fit(X, y, epochs=args.steps * 10)
+    fit_s = time.perf_counter() - t1
+    rep = selector.regret_report(sel, [cs for _, cs in test])
+    rep_train = selector.regret_report(sel, [cs for _, cs in train])
+    out_dir = os.path.join(ROOT, "gpurun_out")
+    os.makedirs(out_dir, exist_ok=True)
+    flat = [(i, j, cs[j][2], cs[j][3], json.dumps(cs[j][0])) for i, (_, cs) in enumerate(data) for j in range(len(cs))]
+    np.savez_compressed(os.path.join(out_dir, "selector_db.npz"),
+                        problem=np.array([a for a, _, _, _, _ in flat]), cand=np.array([b for _, b, _, _, _ in flat]),
+                        features=np.stack([f for _, _, f, _, _ in flat]), ms=np.array([m for _, _, _, m, _ in flat]),
+                        hints=np.array([h for _, _, _, _, h in flat]),
+                        problems=np.frombuffer(json.dumps([p for p, _ in data]).encode(), dtype=np.uint8))
+    value = 100.0 * max(0.0, 1.0 - rep["mlp_regret_mean"])
+    return dict(ms=fit_s * 1e3, value=value, hbm_gbs=0.0, rt_err=None, clocks={"sm_mhz": None, "sm_max_mhz": None,
+                                                                                "reasons": ["not sampled"]},
+                launches=0,
+                extra={"selector": dict(rep, train=rep_train, problems_timed=len(data), train_problems=ntrain,
+                                        candidates_per_problem=float(np.mean([len(cs) for _, cs in data])),
+                                        autotune_s=round(tune_s, 1), fit_s=round(fit_s, 2),
+                                        loss_first=float(hist[0]), loss_last=float(hist[-1]))})
+
+
 def time_reference(wl, threads, transforms, steps, warmup, min_time=None):
     """The reference library's own CPU path (AOCL-FFTZ compiled from its
     sources into oracle/_ref/, OpenMP) through aoclfftz_setup_f/execute on host
@@ -513,6 +566,16 @@ def main():
         if out is not None:
             print(json.dumps(out))
         return
+    if wl.get("selector"):
+        r = run_selector(args, wl)
+        if rank == 0:
+            print(json.dumps({"metric": "learned plan selector regret vs exhaustive autotuning (held-out)",
+                              "value": round(r["value"], 2), "unit": "% of best (100 = always optimal)",
+                              "higher_is_better": True, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": round(r["ms"], 1), "scaling": "weak", "vs_baseline": None,
+                              "dtype": "mixed", "data": "synthetic", "config": {"workload": wl["desc"]},
+                              **r["extra"]}))
+        return
     r = run_ragged(args, wl) if wl.get("ragged") else run_ours(args, wl)
     if rank != 0:
         return
@@ -532,7 +595,7 @@ def main():
     line.update(r.get("extra", {}))
     if "e2e" in r:
         line["e2e"] = r["e2e"]
-    if ws == 1 and not args.no_cpu_baseline and not wl.get("ragged"):
+    if ws == 1 and not args.no_cpu_baseline and not wl.get("ragged") and not wl.get("selector"):
         try:
             line["cpu_baseline"] = cpu_baseline(wl)
         except Exception as e:  # the baseline is reported, never required

@@ -84,6 +84,20 @@ FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFT
                                      const FFTZ_INT64 *out_offsets);
 aoclfftz_error_type aoclfftz_gpu_ragged_execute(FFTZ_VOID *handle, FFTZ_VOID *in, FFTZ_VOID *out);
 
+/* Learned plan selector: an MLP F -> 64 -> 64 -> 1 (ReLU) predicting the log
+ * time of a candidate plan from its features, trained and evaluated by the
+ * library's own CUDA kernels on device buffers. params holds W1[F][64], b1,
+ * W2[64][64], b2, w3[64], b3 (float32). forward needs 2*B*64 floats of work,
+ * grad 4*B*64 + 2*B; grad writes d(mean squared error)/d(params) and the loss
+ * (a device float). adam performs one Adam step (step counts from 1). */
+FFTZ_INT32 aoclfftz_gpu_mlp_nparams(FFTZ_INT32 features);
+FFTZ_INT32 aoclfftz_gpu_mlp_forward(const float *params, FFTZ_INT32 features, const float *x, FFTZ_INT32 batch,
+                                    float *y, float *work, FFTZ_VOID *stream);
+FFTZ_INT32 aoclfftz_gpu_mlp_grad(const float *params, FFTZ_INT32 features, const float *x, const float *target,
+                                 FFTZ_INT32 batch, float *grads, float *loss, float *work, FFTZ_VOID *stream);
+FFTZ_INT32 aoclfftz_gpu_mlp_adam(float *params, const float *grads, float *m, float *v, FFTZ_INT32 n, float lr,
+                                 FFTZ_INT32 step, FFTZ_VOID *stream);
+
 /* Text of the last error recorded by this thread (empty if none). */
 const FFTZ_CHAR *aoclfftz_gpu_last_error(FFTZ_VOID);
 

@@ -32,7 +32,7 @@ def span(dims, vecs, side, n0=None):
 
 
 def run_gpu(dtype, dims, vecs, x_in, out_scalars, fft_type=0, direction=0, placement=1, host=False, ilp64=False,
-            repeat=1, lib=None):
+            repeat=1, lib=None, pinned=False):
     """Executes one problem on the GPU through aoclfftz_setup_* / execute.
 
     x_in: raw input buffer (numpy; viewed as the real scalar type).
@@ -45,7 +45,21 @@ def run_gpu(dtype, dims, vecs, x_in, out_scalars, fft_type=0, direction=0, place
     xin = np.ascontiguousarray(x_in).view(real).ravel()
     tdt = torch.float32 if dtype == "f32" else torch.float64
     outs = []
-    if host:
+    if host and pinned:
+        # page-locked host memory: the library pipelines copy-in / passes / copy-out
+        if placement == 0:
+            t = torch.zeros(max(xin.size, out_scalars), dtype=tdt).pin_memory()
+            buf = t.numpy()
+            buf[: xin.size] = xin
+            pin = pout = buf.ctypes.data
+            hold = [buf, t]
+        else:
+            ti = torch.from_numpy(xin.copy()).pin_memory()
+            to = torch.zeros(out_scalars, dtype=tdt).pin_memory()
+            hin, hout = ti.numpy(), to.numpy()
+            pin, pout = hin.ctypes.data, hout.ctypes.data
+            hold = [hin, hout, ti, to]
+    elif host:
         if placement == 0:
             buf = np.zeros(max(xin.size, out_scalars), dtype=real)
             buf[: xin.size] = xin

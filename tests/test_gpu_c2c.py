@@ -31,7 +31,8 @@ def bound(dims, dtype):
     return oracle.tol(N, dtype)
 
 
-def check_c2c(dtype, dims, vecs, direction=0, placement=1, seed=1, host=False, compare_ref=True, ilp64=False):
+def check_c2c(dtype, dims, vecs, direction=0, placement=1, seed=1, host=False, compare_ref=True, ilp64=False,
+              pinned=False):
     rank = len(dims)
     lshape = [v[0] for v in reversed(vecs)] + [d[0] for d in reversed(dims)]
     total = int(np.prod(lshape))
@@ -39,7 +40,8 @@ def check_c2c(dtype, dims, vecs, direction=0, placement=1, seed=1, host=False, c
     in_sc = 2 * span(dims, vecs, "in")
     out_sc = 2 * span(dims, vecs, "out")
     raw_in = scatter(x, [(d[0], d[1]) for d in dims], [(v[0], v[1]) for v in vecs], in_sc, dtype)
-    out_raw, plan = run_gpu(dtype, dims, vecs, raw_in, out_sc, 0, direction, placement, host=host, ilp64=ilp64)
+    out_raw, plan = run_gpu(dtype, dims, vecs, raw_in, out_sc, 0, direction, placement, host=host, ilp64=ilp64,
+                            pinned=pinned)
     y = gather(out_raw, [(d[0], d[2]) for d in dims], [(v[0], v[2]) for v in vecs], dtype)
     ref = oracle_c2c(x, rank, -1 if direction == 0 else +1)
     err = oracle.rel_l2(y, ref)
@@ -119,6 +121,17 @@ def test_host_buffers_and_ilp64():
     check_c2c("f32", [(1024, 1, 1)], [(8, 1024, 1024)], 0, host=True)
     check_c2c("f64", [(100, 1, 1)], [(3, 100, 100)], 1, host=True, placement=0)
     check_c2c("f64", [(512, 1, 1)], [(2, 512, 512)], 0, ilp64=True)
+
+
+def test_pinned_host_buffers_pipelined():
+    """Page-locked host buffers take the chunked copy-in / passes / copy-out
+    pipeline (three streams); results must match the oracle exactly as the
+    device path does."""
+    check_c2c("f32", [(4096, 1, 1)], [(64, 4096, 4096)], 0, host=True, pinned=True, compare_ref=False)
+    check_c2c("f64", [(1 << 18, 1, 1)], [(4, 1 << 18, 1 << 18)], 1, host=True, pinned=True, compare_ref=False)
+    check_c2c("f32", [(100, 1, 1)], [(48, 130, 100)], 0, host=True, pinned=True)
+    check_c2c("f64", [(256, 1, 1)], [(12, 256, 256)], 1, placement=0, host=True, pinned=True)
+    check_c2c("f32", [(16, 1, 1), (8, 16, 16)], [(6, 128, 128)], 0, host=True, pinned=True)
 
 
 def test_size_one_and_empty_batch():

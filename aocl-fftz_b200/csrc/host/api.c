@@ -391,12 +391,21 @@ static int prepare_chunks(fz_plan *pl)
         if (pl->sv_vecs[i].is > pl->sv_vecs[o].is) o = i;
     const fz_dim outer = pl->sv_vecs[o];
     if (outer.n < 2) return -1;
+    /* everything below the outer dimension must fit inside one outer stride on
+     * both sides, so that chunks are disjoint byte ranges */
+    int64_t span_in = 1, span_out = 1;
     for (int i = 0; i < pl->sv_rank; i++)
-        if (pl->sv_dims[i].is * pl->sv_dims[i].n > outer.is || pl->sv_dims[i].os * pl->sv_dims[i].n > outer.os)
-            return -1;
+    {
+        span_in += (pl->sv_dims[i].n - 1) * pl->sv_dims[i].is;
+        span_out += (pl->sv_dims[i].n - 1) * pl->sv_dims[i].os;
+    }
     for (int i = 0; i < pl->sv_vrank; i++)
-        if (i != o && (pl->sv_vecs[i].is * pl->sv_vecs[i].n > outer.is || pl->sv_vecs[i].os * pl->sv_vecs[i].n > outer.os))
-            return -1;
+        if (i != o && pl->sv_vecs[i].n > 0)
+        {
+            span_in += (pl->sv_vecs[i].n - 1) * pl->sv_vecs[i].is;
+            span_out += (pl->sv_vecs[i].n - 1) * pl->sv_vecs[i].os;
+        }
+    if (span_in > outer.is || span_out > outer.os) return -1;
     /* about 8 chunks of at least 4 MiB each */
     const int64_t per_entry = pl->in_bytes / outer.n + 1;
     int64_t target = outer.n / 8;
@@ -433,6 +442,9 @@ static int prepare_chunks(fz_plan *pl)
     g_hints = saved;
     if (!ch) return -1;
     ch->stream = NULL;
+    /* the chunk plan's passes run on the slot buffers below, not on its own scratch */
+    if (ch->scratch) cudaFree(ch->scratch);
+    ch->scratch = NULL;
     const int64_t esz_in = (pl->fft_type == 0 || pl->direction == 1) ? (pl->dtype == 0 ? 8 : 16) : (pl->dtype == 0 ? 4 : 8);
     const int64_t esz_out = (pl->fft_type == 0 || pl->direction == 0) ? (pl->dtype == 0 ? 8 : 16) : (pl->dtype == 0 ? 4 : 8);
     pl->chunk = ch;

@@ -6,7 +6,10 @@ in place on an array of R complex values held in registers. The backward
 transform is obtained by the kernels through conjugation of the input and the
 output, so only the forward codelets are generated.
 
-* R = 2, 4, 8, 16: radix-2 decimation-in-time network; twiddles W_R^k with
+* R = 2, 4, 8, 16: split-radix decimation-in-time network,
+  X[k] = E[k] + W^k O1[k] + W^3k O3[k] with E the half-length DFT of the even
+  inputs and O1, O3 the quarter-length DFTs of inputs 1 and 3 mod 4, which
+  needs fewer real operations than the radix-2 network; twiddles W_R^k with
   k in {0, R/4} are applied as sign swaps, k in {R/8, 3R/8} with one
   multiply by sqrt(1/2) per component.
 * R = 3, 5, 7, 11, 13: the symmetric-pair form
@@ -43,6 +46,60 @@ class Emitter:
         self.count += 1
         self.lines.append("    const T %s_r = %s, %s_i = %s;" % (name, expr_re, name, expr_im))
         return name
+
+
+def twiddle(em, o, m, n):
+    """(re, im) expressions of W_n^m * o, W = exp(-2 pi i / n)."""
+    m %= n
+    if m == 0:
+        return "%s_r" % o, "%s_i" % o
+    if 4 * m == n:  # -i
+        return "%s_i" % o, "-%s_r" % o
+    if 8 * m == n:  # (1 - i)/sqrt2
+        h = lit(mpmath.sqrt(2) / 2)
+        t = em.tmp("%s * (%s_r + %s_i)" % (h, o, o), "%s * (%s_i - %s_r)" % (h, o, o))
+        return "%s_r" % t, "%s_i" % t
+    if 8 * m == 3 * n:  # -(1 + i)/sqrt2
+        h = lit(mpmath.sqrt(2) / 2)
+        t = em.tmp("%s * (%s_i - %s_r)" % (h, o, o), "-%s * (%s_r + %s_i)" % (h, o, o))
+        return "%s_r" % t, "%s_i" % t
+    ang = 2 * mpmath.pi * m / n
+    c, s = lit(mpmath.cos(ang)), lit(mpmath.sin(ang))
+    # (or + i oi)(c - i s) = (or c + oi s) + i (oi c - or s)
+    t = em.tmp("fma(%s, %s_r, %s * %s_i)" % (c, o, s, o), "fma(%s, %s_i, -(%s * %s_r))" % (c, o, s, o))
+    return "%s_r" % t, "%s_i" % t
+
+
+def gen_pow2_split(R):
+    em = Emitter()
+
+    def rec(idx):
+        n = len(idx)
+        if n == 1:
+            return [em.tmp("v[%d].x" % idx[0], "v[%d].y" % idx[0])]
+        if n == 2:
+            a, b = rec(idx[:1]), rec(idx[1:])
+            return [em.tmp("%s_r + %s_r" % (a[0], b[0]), "%s_i + %s_i" % (a[0], b[0])),
+                    em.tmp("%s_r - %s_r" % (a[0], b[0]), "%s_i - %s_i" % (a[0], b[0]))]
+        e = rec(idx[0::2])
+        o1 = rec(idx[1::4])
+        o3 = rec(idx[3::4])
+        q = n // 4
+        out = [None] * n
+        for k in range(q):
+            ar, ai = twiddle(em, o1[k], k, n)
+            br, bi = twiddle(em, o3[k], 3 * k, n)
+            sm = em.tmp("%s + %s" % (ar, br), "%s + %s" % (ai, bi))
+            df = em.tmp("%s - %s" % (ar, br), "%s - %s" % (ai, bi))
+            out[k] = em.tmp("%s_r + %s_r" % (e[k], sm), "%s_i + %s_i" % (e[k], sm))
+            out[k + 2 * q] = em.tmp("%s_r - %s_r" % (e[k], sm), "%s_i - %s_i" % (e[k], sm))
+            # E[k + n/4] -/+ i d
+            out[k + q] = em.tmp("%s_r + %s_i" % (e[k + q], df), "%s_i - %s_r" % (e[k + q], df))
+            out[k + 3 * q] = em.tmp("%s_r - %s_i" % (e[k + q], df), "%s_i + %s_r" % (e[k + q], df))
+        return out
+
+    outs = rec(list(range(R)))
+    return em.lines + ["    v[%d].x = %s_r; v[%d].y = %s_i;" % (k, o, k, o) for k, o in enumerate(outs)]
 
 
 def gen_pow2(R):
@@ -128,7 +185,7 @@ def main():
     out.append("namespace fftz {")
     out.append("template <int R> struct Dft;")
     for R in sorted(RADICES_POW2 + RADICES_ODD):
-        body = gen_pow2(R) if R in RADICES_POW2 else gen_odd(R)
+        body = gen_pow2_split(R) if R in RADICES_POW2 else gen_odd(R)
         out.append("template <> struct Dft<%d> {" % R)
         out.append("  template <typename T, typename T2>")
         out.append("  static __device__ __forceinline__ void apply(T2 (&v)[%d]) {" % R)

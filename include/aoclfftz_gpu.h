@@ -101,6 +101,26 @@ FFTZ_INT32 aoclfftz_gpu_mlp_adam(float *params, const float *grads, float *m, fl
 /* Text of the last error recorded by this thread (empty if none). */
 const FFTZ_CHAR *aoclfftz_gpu_last_error(FFTZ_VOID);
 
+/* No-allocation execute. No counterpart in the reference, which never needs
+ * device memory. For callers that may not allocate device memory when they
+ * transform: another allocator owns the device's memory, or a latency-critical
+ * loop cannot afford cudaFree's device-wide synchronisation. Runs howmany
+ * contiguous single-precision complex transforms of length n (distance n)
+ * from device buffer `in` to device buffer `out` (in == out allowed), forward
+ * (direction 0) or unnormalised backward (1), on `stream`, with the plan
+ * path's four-step kernels and their intermediate in a 32 MiB static device
+ * array. n must be a power of two in [2^15, 2^22] and n * howmany at most
+ * 2^22; anything else returns AOCLFFTZ_INVALID_INPUT with a message in
+ * aoclfftz_gpu_last_error. Calls no cudaMalloc, cudaFree or other allocating
+ * routine. The first call on each device sets up that device's tables and
+ * waits for them on `stream`; make it before any stream capture begins
+ * (during capture it returns AOCLFFTZ_SETUP_FAILURE). All calls on a device
+ * share the one scratch array: calls whose kernels overlap on the GPU race,
+ * so order them on one stream. */
+aoclfftz_error_type aoclfftz_gpu_execute_noalloc_c2c_f(const FFTZ_VOID *in, FFTZ_VOID *out, FFTZ_INT64 n,
+                                                       FFTZ_INT64 howmany, FFTZ_INT32 direction,
+                                                       FFTZ_VOID *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,12 +59,14 @@ typedef struct fz_ragged
     int64_t count, npasses, nitems;
     int64_t in_elems, out_elems; /* complex elements the buffers span */
     void *d_passes, *d_items, *d_done, *d_queue, *d_err;
+    void *d_ind;                  /* per-transform element offsets of grouped passes */
+    int64_t ngroups;
     int grid, smem;
     void *cap_stream;             /* stream used to capture the graph */
     void *graph, *graph_exec;     /* cudaGraph_t / cudaGraphExec_t */
     const void *g_in;             /* buffers the graph was captured with */
     void *g_out;
-    char summary[160];
+    char summary[224];
 } fz_ragged;
 
 typedef struct fz_plan

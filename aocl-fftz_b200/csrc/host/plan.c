@@ -99,6 +99,17 @@ static int64_t absl(int64_t x) { return x < 0 ? -x : x; }
 /* every pass on the generic kernel (the persistent executor runs only that) */
 static int generic_only(const fz_plan *pl) { return pl->hints.kernel_family == 3; }
 
+/* kernel_family 4: passes for the persistent ragged executor, whose CTAs have
+ * 256 threads: compile-time kernels up to length 4096, never the pipelined
+ * family */
+static int ragged_mode(const fz_plan *pl) { return pl->hints.kernel_family == 4; }
+static int64_t fast_max_n(const fz_plan *pl)
+{
+    const int64_t m = fftz_fast_max_n(pl->dtype);
+    return ragged_mode(pl) && m > 4096 ? 4096 : m;
+}
+static int fast_max_threads(const fz_plan *pl) { return ragged_mode(pl) ? 256 : (pl->dtype == 0 ? 1024 : 512); }
+
 /* Batch dims: optionally sorted by stride (smallest first, so that bdim[0]
  * is the one lanes may run along), then adjacent dims merged when they form
  * one arithmetic progression on both sides (the reference's fuse_vecs,
@@ -214,13 +225,13 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
     p->dst = dst;
     if (set_batch(k, b, nb, keep_first)) return NULL;
     set_modes(k);
-    const int fast = !generic_only(pl) && is_pow2(n) && n >= 2 && n <= fftz_fast_max_n(pl->dtype);
+    const int fast = !generic_only(pl) && is_pow2(n) && n >= 2 && n <= fast_max_n(pl);
     int maxthr;
     if (fast)
     {
         k->nstages = fftz_fast_radices((int)n, k->radix);
         k->tpt = fftz_fast_tpt((int)n);
-        maxthr = pl->dtype == 0 ? 1024 : 512;
+        maxthr = fast_max_threads(pl);
         if (k->nstages == 1 && k->in_mode != k->out_mode) k->out_mode = k->in_mode;
         int tabs = (variant_bits & 2) != 0, tw4 = (flags & FFTZ_F_TW4) != 0;
         const int fam = pl->hints.kernel_family;
@@ -277,7 +288,7 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
     {
         /* two slots do not fit: the one-tile-per-CTA kernel of the same shape */
         k->variant = k->variant == FFTZ_VAR_PIPE_TW4 ? FFTZ_VAR_FAST_TW4 : FFTZ_VAR_FAST;
-        maxthr = pl->dtype == 0 ? 1024 : 512;
+        maxthr = fast_max_threads(pl);
         finish_launch_shape(pl, k, nslots, maxthr);
     }
     if (fftz_pass_smem_bytes(k) > fftz_smem_limit())
@@ -299,7 +310,7 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
 static int single_pass_ok(const fz_plan *pl, int64_t n)
 {
     if (n == 1) return 1;
-    if (!generic_only(pl) && is_pow2(n) && n <= fftz_fast_max_n(pl->dtype)) return 1;
+    if (!generic_only(pl) && is_pow2(n) && n <= fast_max_n(pl)) return 1;
     int32_t r[FFTZ_MAX_STAGES];
     int s = generic_radices(n, r);
     if (s < 0) return 0;
@@ -314,7 +325,7 @@ static int single_pass_ok(const fz_plan *pl, int64_t n)
  * core/common/pow2_radix_decompose.c:15-35) */
 static int splittable(const fz_plan *pl, int64_t n)
 {
-    const int64_t m = fftz_fast_max_n(pl->dtype);
+    const int64_t m = fast_max_n(pl);
     return single_pass_ok(pl, n) || (smooth13(n) && n <= m * m);
 }
 
@@ -592,7 +603,7 @@ static int add_line(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_d
     if (algo == 3 && n > 1) return bluestein(pl, n, ies, oes, b, nb, src, dst);
     if (algo != 2 && single_pass_ok(pl, n))
         return line_pass(pl, n, ies, oes, b, nb, 0, src, dst, flags, 0) ? 0 : -1;
-    if (smooth13(n) && n <= (int64_t)fftz_fast_max_n(pl->dtype) * fftz_fast_max_n(pl->dtype))
+    if (smooth13(n) && n <= fast_max_n(pl) * fast_max_n(pl))
     {
         if (src == dst)
         {

@@ -4,11 +4,14 @@
  *
  * The reference has no ragged API: its callers run one plan per length
  * back to back (AOCL-FFTZ executes each plan's solver tree,
- * core/executor.c:17-44). Here every transform is planned with the ordinary
- * planner restricted to the generic kernel, its passes are flattened into a
- * table of CTA tiles (pass, tile, predecessor pass), and the persistent
- * executor (kernels/fft_ragged.cu) runs the whole table. Tiles are ordered by
- * pass depth, then by decreasing length (largest first balances the tail).
+ * core/executor.c:17-44). Here the transforms are grouped by length; each
+ * group is planned once by the ordinary planner (in its executor mode:
+ * 256-thread tiles, compile-time kernels up to length 4096) as a batch whose
+ * transform dimension is indirect, so the group's transforms keep their own
+ * offsets in the packed buffers. The passes are flattened into a table of CTA
+ * tiles (pass, tile, predecessor pass) and the persistent executor
+ * (kernels/fft_ragged.cu) runs the whole table. Tiles are ordered by pass
+ * depth, then by decreasing length (largest first balances the tail).
  */
 #include <cuda_runtime_api.h>
 #include <stdio.h>
@@ -17,6 +20,8 @@
 
 #include "aoclfftz_gpu.h"
 #include "fz_internal.h"
+
+#define FZ_MAX_PASSES_RG 64
 
 typedef struct
 {
@@ -45,6 +50,7 @@ void fz_ragged_free(fz_ragged *rg)
     cudaFree(rg->d_done);
     cudaFree(rg->d_queue);
     cudaFree(rg->d_err);
+    cudaFree(rg->d_ind);
     free(rg);
 }
 
@@ -68,6 +74,230 @@ static void resolve(int id, int64_t io_off_bytes, const int64_t *soff, int32_t *
     }
 }
 
+#define RG_THREADS 256
+
+/* Launch shape of one pass inside the executor (256-thread CTAs): a
+ * compile-time tile with tpc * tpt == 256 where the executor has one,
+ * otherwise the generic tile with as many transforms as fit (loads and stores
+ * through the generic phases, which know every table and bound). */
+static int ragged_shape(fftz_pass_t *k, int dtype, int64_t smem_cap)
+{
+    const int nslots = k->n > k->nload ? k->n : k->nload;
+    const int colmap = k->in_mode == 1 || k->out_mode == 1;
+    const int fastv = k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4 ||
+                      k->variant == FFTZ_VAR_FAST_TABS || k->variant == FFTZ_VAR_FAST_TW4_TABS ||
+                      k->variant == FFTZ_VAR_FAST_BLUE;
+    if (fastv && fftz_ragged_fast_ok(k->n, k->variant) && k->tpt <= RG_THREADS && RG_THREADS % k->tpt == 0)
+    {
+        fftz_pass_t t = *k;
+        t.tpc = RG_THREADS / t.tpt;
+        t.sstride = colmap ? fftz_smem_stride_cols(dtype, nslots, t.tpc) : fftz_smem_stride(dtype, nslots);
+        if (fftz_pass_smem_bytes(&t) <= smem_cap)
+        {
+            *k = t;
+            return 0;
+        }
+    }
+    if (k->variant != FFTZ_VAR_GENERIC)
+    {
+        k->variant = FFTZ_VAR_GENERIC;
+        k->fuse_load = 0;
+        k->fuse_store = 0;
+    }
+    if (k->tpt < 1 || k->tpt > RG_THREADS) return -1;
+    for (int tpc = RG_THREADS / k->tpt; tpc >= 1; tpc--)
+    {
+        k->tpc = tpc;
+        k->sstride = colmap ? fftz_smem_stride_cols(dtype, nslots, tpc) : fftz_smem_stride(dtype, nslots);
+        if (fftz_pass_smem_bytes(k) <= smem_cap) return 0;
+    }
+    return -1;
+}
+
+typedef struct
+{
+    fz_plan *pl;
+    int dtype, direction;
+    int64_t csz, smem_cap;
+    int64_t npass, cap_pass, cap_aux, nitem, cap_item, scratch_total, nind, cap_ind;
+    fftz_pass_t *passes;
+    int64_t (*toff)[7];  /* per pass: table offsets in the merged blob */
+    int64_t (*indpos)[2]; /* per pass: positions of its in / out offset lists, -1 if none */
+    int64_t *ind;         /* host copy of every offset list */
+    fz_item_sort *items;
+} rg_build;
+
+static int grow(void **p, int64_t *cap, int64_t need, size_t esz, int64_t first)
+{
+    if (need <= *cap) return 0;
+    int64_t nc = *cap ? *cap : first;
+    while (nc < need) nc *= 2;
+    void *np = realloc(*p, esz * (size_t)nc);
+    if (!np) return -1;
+    *p = np;
+    *cap = nc;
+    return 0;
+}
+
+/* Plans c transforms of length n whose element offsets are tin[] / tout[] and
+ * appends their passes and tiles. With c >= 2 the transform dimension of the
+ * plan becomes the indirect batch dimension of each pass that reads the input
+ * or writes the output. Returns 1 when the plan's passes do not expose that
+ * dimension (the caller then plans the transforms one by one), -1 on error. */
+static int add_group(rg_build *B, int64_t n, int64_t c, const int64_t *tin, const int64_t *tout)
+{
+    const int64_t big = 2 * n + 1; /* a batch stride no other dimension can continue */
+    fz_plan sub;
+    memset(&sub, 0, sizeof(sub));
+    sub.dtype = B->dtype;
+    sub.direction = B->direction;
+    sub.placement = 1;
+    sub.hints.kernel_family = 4;
+    fz_dim d = {n, 1, 1}, v = {c, c > 1 ? big : n, c > 1 ? big : n};
+    if (fz_plan_build(&sub, 1, &d, 1, &v))
+    {
+        free(sub.pass);
+        free(sub.blob.p);
+        return -1;
+    }
+    int rc = 0;
+    int32_t inddim[FZ_MAX_PASSES_RG];
+    if (sub.npass > FZ_MAX_PASSES_RG) rc = 1;
+    /* every pass must be plain c2c, and the indirect dimension must be found */
+    for (int j = 0; j < sub.npass && rc == 0; j++)
+    {
+        fz_pass *sp = &sub.pass[j];
+        if (sp->is_elem)
+        {
+            rc = 1;
+            break;
+        }
+        inddim[j] = -1;
+        if (c < 2) continue;
+        const fftz_pass_t *k = &sp->k;
+        const int need_in = sp->src == FZ_BUF_IN, need_out = sp->dst == FZ_BUF_OUT;
+        if (!need_in && !need_out) continue;
+        for (int q = 0; q < k->nbdims; q++)
+            if (k->bdim[q] == c && (!need_in || k->ibs[q] == big) && (!need_out || k->obs[q] == big)) inddim[j] = q;
+        if (inddim[j] < 0) rc = 1;
+    }
+    if (rc)
+    {
+        free(sub.pass);
+        free(sub.blob.p);
+        return rc;
+    }
+    int64_t boff = 0;
+    if (sub.blob.len)
+    {
+        boff = fz_blob_add(&B->pl->blob, sub.blob.p, sub.blob.len);
+        if (boff < 0) rc = -1;
+    }
+    int64_t soff[FZ_MAX_SCRATCH];
+    for (int q = 0; q < sub.nscratch; q++)
+    {
+        soff[q] = B->scratch_total;
+        B->scratch_total += (sub.scratch_elems[q] * B->csz + 255) & ~(int64_t)255;
+    }
+    /* offset lists of this group */
+    int64_t pin = -1, pout = -1;
+    if (rc == 0 && c > 1)
+    {
+        if (grow((void **)&B->ind, &B->cap_ind, B->nind + 2 * c, sizeof(int64_t), 4096))
+            rc = -1;
+        else
+        {
+            pin = B->nind;
+            memcpy(B->ind + pin, tin, sizeof(int64_t) * (size_t)c);
+            pout = pin + c;
+            memcpy(B->ind + pout, tout, sizeof(int64_t) * (size_t)c);
+            B->nind += 2 * c;
+        }
+    }
+    int64_t prev_nblk = 0;
+    for (int j = 0; j < sub.npass && rc == 0; j++)
+    {
+        fz_pass *sp = &sub.pass[j];
+        if (grow((void **)&B->passes, &B->cap_pass, B->npass + 1, sizeof(fftz_pass_t), 1024))
+        {
+            rc = -1;
+            break;
+        }
+        if (B->cap_aux < B->cap_pass)
+        {
+            void *a = realloc(B->toff, sizeof(int64_t) * 7 * (size_t)B->cap_pass);
+            if (a) B->toff = (int64_t(*)[7])a;
+            void *b = a ? realloc(B->indpos, sizeof(int64_t) * 2 * (size_t)B->cap_pass) : NULL;
+            if (b) B->indpos = (int64_t(*)[2])b;
+            if (!a || !b)
+            {
+                rc = -1;
+                break;
+            }
+            B->cap_aux = B->cap_pass;
+        }
+        fftz_pass_t k = sp->k;
+        const int64_t io = c > 1 ? 0 : tin[0] * B->csz, oo = c > 1 ? 0 : tout[0] * B->csz;
+        int64_t ioff, ooff;
+        resolve(sp->src, io + sp->in_off, soff, &k.src_buf, &ioff);
+        resolve(sp->dst, oo + sp->out_off, soff, &k.dst_buf, &ooff);
+        if (k.src_buf == FFTZ_RBUF_SCRATCH) ioff += sp->in_off;
+        if (k.dst_buf == FFTZ_RBUF_SCRATCH) ooff += sp->out_off;
+        k.in = (const void *)(size_t)ioff;
+        k.out = (void *)(size_t)ooff;
+        k.ind_dim = inddim[j] >= 0 ? inddim[j] : 0;
+        k.ind_in = NULL;
+        k.ind_out = NULL;
+        if (ragged_shape(&k, B->dtype, B->smem_cap))
+        {
+            fz_set_error("ragged setup: a pass of length %d does not fit the executor", k.n);
+            rc = -1;
+            break;
+        }
+        const int64_t o7[7] = {sp->off_tw, sp->off_tw4hi, sp->off_tw4lo, sp->off_pre, sp->off_post, sp->off_mid,
+                               sp->off_rtw};
+        for (int t = 0; t < 7; t++) B->toff[B->npass][t] = o7[t] >= 0 ? boff + o7[t] : -1;
+        B->indpos[B->npass][0] = (inddim[j] >= 0 && sp->src == FZ_BUF_IN) ? pin : -1;
+        B->indpos[B->npass][1] = (inddim[j] >= 0 && sp->dst == FZ_BUF_OUT) ? pout : -1;
+        B->passes[B->npass] = k;
+        const int64_t nblk = (k.ntf + k.tpc - 1) / k.tpc;
+        if (grow((void **)&B->items, &B->cap_item, B->nitem + nblk, sizeof(fz_item_sort), 4096))
+        {
+            rc = -1;
+            break;
+        }
+        for (int64_t b = 0; b < nblk; b++)
+        {
+            fz_item_sort *it = &B->items[B->nitem++];
+            it->it.pass = (int32_t)B->npass;
+            it->it.dep = j > 0 ? (int32_t)(B->npass - 1) : -1;
+            it->it.blk = b;
+            it->it.dep_count = j > 0 ? prev_nblk : 0;
+            it->it.signal = j + 1 < sub.npass;
+            it->it.pad_ = 0;
+            it->depth = j;
+            it->cost = n;
+        }
+        prev_nblk = nblk;
+        B->npass++;
+    }
+    free(sub.pass);
+    free(sub.blob.p);
+    return rc;
+}
+
+typedef struct
+{
+    int64_t n, idx;
+} rg_size;
+
+static int size_cmp(const void *a, const void *b)
+{
+    const rg_size *x = (const rg_size *)a, *y = (const rg_size *)b;
+    if (x->n != y->n) return x->n < y->n ? -1 : 1;
+    return x->idx < y->idx ? -1 : (x->idx > y->idx);
+}
+
 FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFTZ_INT64 count,
                                      const FFTZ_INT64 *sizes, const FFTZ_INT64 *in_offsets,
                                      const FFTZ_INT64 *out_offsets)
@@ -77,13 +307,17 @@ FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFT
         fz_set_error("ragged setup: invalid arguments");
         return NULL;
     }
+    rg_build B;
+    memset(&B, 0, sizeof(B));
     fz_plan *pl = (fz_plan *)calloc(1, sizeof(fz_plan));
     fz_ragged *rg = (fz_ragged *)calloc(1, sizeof(fz_ragged));
-    int64_t npass = 0, cap_pass = 0, nitem = 0, cap_item = 0, scratch_total = 0;
-    fftz_pass_t *passes = NULL;
-    int64_t(*toff)[7] = NULL; /* per pass: table offsets in the merged blob */
-    fz_item_sort *items = NULL;
-    if (!pl || !rg) goto fail_mem;
+    rg_size *ord = (rg_size *)malloc(sizeof(rg_size) * (size_t)count);
+    int64_t *tin = (int64_t *)malloc(sizeof(int64_t) * (size_t)count);
+    int64_t *tout = (int64_t *)malloc(sizeof(int64_t) * (size_t)count);
+    int64_t *gin = (int64_t *)malloc(sizeof(int64_t) * (size_t)count);
+    int64_t *gout = (int64_t *)malloc(sizeof(int64_t) * (size_t)count);
+    fftz_ritem_t *flat = NULL;
+    if (!pl || !rg || !ord || !tin || !tout || !gin || !gout) goto fail_mem;
     pl->magic = FZ_MAGIC;
     pl->dtype = dtype;
     pl->direction = direction;
@@ -95,7 +329,11 @@ FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFT
         fz_set_error("no CUDA device available");
         goto fail;
     }
-    const int64_t csz = dtype == 0 ? 8 : 16;
+    B.pl = pl;
+    B.dtype = dtype;
+    B.direction = direction;
+    B.csz = dtype == 0 ? 8 : 16;
+    B.smem_cap = dtype == 0 ? 72 * 1024 : 100 * 1024;
     int64_t next_in = 0, next_out = 0;
     for (int64_t i = 0; i < count; i++)
     {
@@ -105,160 +343,91 @@ FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFT
             fz_set_error("ragged setup: transform %lld has length %lld", (long long)i, (long long)n);
             goto fail;
         }
-        const int64_t io = in_offsets ? in_offsets[i] : next_in;
-        const int64_t oo = out_offsets ? out_offsets[i] : next_out;
-        next_in = io + n;
-        next_out = oo + n;
-        if (io + n > rg->in_elems) rg->in_elems = io + n;
-        if (oo + n > rg->out_elems) rg->out_elems = oo + n;
-        fz_plan sub;
-        memset(&sub, 0, sizeof(sub));
-        sub.dtype = dtype;
-        sub.direction = direction;
-        sub.placement = 1;
-        sub.hints.kernel_family = 3;
-        fz_dim d = {n, 1, 1}, v = {1, n, n};
-        if (fz_plan_build(&sub, 1, &d, 1, &v))
+        tin[i] = in_offsets ? in_offsets[i] : next_in;
+        tout[i] = out_offsets ? out_offsets[i] : next_out;
+        next_in = tin[i] + n;
+        next_out = tout[i] + n;
+        if (tin[i] + n > rg->in_elems) rg->in_elems = tin[i] + n;
+        if (tout[i] + n > rg->out_elems) rg->out_elems = tout[i] + n;
+        ord[i].n = n;
+        ord[i].idx = i;
+    }
+    /* one batched plan per distinct length */
+    qsort(ord, (size_t)count, sizeof(rg_size), size_cmp);
+    for (int64_t g0 = 0; g0 < count;)
+    {
+        int64_t g1 = g0;
+        while (g1 < count && ord[g1].n == ord[g0].n) g1++;
+        const int64_t c = g1 - g0;
+        for (int64_t q = 0; q < c; q++)
         {
-            free(sub.pass);
-            free(sub.blob.p);
+            gin[q] = tin[ord[g0 + q].idx];
+            gout[q] = tout[ord[g0 + q].idx];
+        }
+        int rc = add_group(&B, ord[g0].n, c, gin, gout);
+        if (rc > 0 && c > 1)
+            for (int64_t q = 0; q < c && rc >= 0; q++) rc = add_group(&B, ord[g0].n, 1, gin + q, gout + q);
+        if (rc > 0)
+        {
+            fz_set_error("ragged setup: length %lld has no executor plan", (long long)ord[g0].n);
             goto fail;
         }
-        int64_t boff = 0;
-        if (sub.blob.len)
-        {
-            boff = fz_blob_add(&pl->blob, sub.blob.p, sub.blob.len);
-            if (boff < 0)
-            {
-                free(sub.pass);
-                free(sub.blob.p);
-                goto fail_mem;
-            }
-        }
-        int64_t soff[FZ_MAX_SCRATCH];
-        for (int k = 0; k < sub.nscratch; k++)
-        {
-            soff[k] = scratch_total;
-            scratch_total += (sub.scratch_elems[k] * csz + 255) & ~(int64_t)255;
-        }
-        int64_t prev_nblk = 0;
-        for (int j = 0; j < sub.npass; j++)
-        {
-            fz_pass *sp = &sub.pass[j];
-            if (sp->is_elem)
-            {
-                fz_set_error("ragged setup: unexpected elementwise pass");
-                free(sub.pass);
-                free(sub.blob.p);
-                goto fail;
-            }
-            if (npass == cap_pass)
-            {
-                cap_pass = cap_pass ? 2 * cap_pass : 1024;
-                fftz_pass_t *np = (fftz_pass_t *)realloc(passes, sizeof(fftz_pass_t) * (size_t)cap_pass);
-                int64_t(*nt)[7] = (int64_t(*)[7])realloc(toff, sizeof(int64_t) * 7 * (size_t)cap_pass);
-                if (!np || !nt)
-                {
-                    free(np ? np : passes);
-                    passes = NULL;
-                    free(nt ? (void *)nt : (void *)toff);
-                    toff = NULL;
-                    free(sub.pass);
-                    free(sub.blob.p);
-                    goto fail_mem;
-                }
-                passes = np;
-                toff = nt;
-            }
-            fftz_pass_t k = sp->k;
-            int64_t ioff, ooff;
-            resolve(sp->src, io * csz + sp->in_off, soff, &k.src_buf, &ioff);
-            resolve(sp->dst, oo * csz + sp->out_off, soff, &k.dst_buf, &ooff);
-            if (k.src_buf == FFTZ_RBUF_SCRATCH) ioff += sp->in_off;
-            if (k.dst_buf == FFTZ_RBUF_SCRATCH) ooff += sp->out_off;
-            k.in = (const void *)(size_t)ioff;
-            k.out = (void *)(size_t)ooff;
-            const int64_t o7[7] = {sp->off_tw, sp->off_tw4hi, sp->off_tw4lo, sp->off_pre, sp->off_post, sp->off_mid,
-                                   sp->off_rtw};
-            for (int t = 0; t < 7; t++) toff[npass][t] = o7[t] >= 0 ? boff + o7[t] : -1;
-            passes[npass] = k;
-            const int64_t nblk = (k.ntf + k.tpc - 1) / k.tpc;
-            for (int64_t b = 0; b < nblk; b++)
-            {
-                if (nitem == cap_item)
-                {
-                    cap_item = cap_item ? 2 * cap_item : 4096;
-                    fz_item_sort *ni = (fz_item_sort *)realloc(items, sizeof(fz_item_sort) * (size_t)cap_item);
-                    if (!ni)
-                    {
-                        free(sub.pass);
-                        free(sub.blob.p);
-                        goto fail_mem;
-                    }
-                    items = ni;
-                }
-                fz_item_sort *it = &items[nitem++];
-                it->it.pass = (int32_t)npass;
-                it->it.dep = j > 0 ? (int32_t)(npass - 1) : -1;
-                it->it.blk = b;
-                it->it.dep_count = j > 0 ? prev_nblk : 0;
-                it->depth = j;
-                it->cost = n;
-            }
-            prev_nblk = nblk;
-            npass++;
-        }
-        free(sub.pass);
-        free(sub.blob.p);
+        if (rc < 0) goto fail;
+        rg->ngroups++;
+        g0 = g1;
     }
-    qsort(items, (size_t)nitem, sizeof(fz_item_sort), item_cmp);
-    /* device state: tables, pass table, item table, counters, scratch */
+    qsort(B.items, (size_t)B.nitem, sizeof(fz_item_sort), item_cmp);
+    /* device state: tables, offset lists, pass table, item table, counters, scratch */
     if (pl->blob.len &&
         (cudaMalloc(&pl->dtab, pl->blob.len) != cudaSuccess ||
          cudaMemcpy(pl->dtab, pl->blob.p, pl->blob.len, cudaMemcpyHostToDevice) != cudaSuccess))
         goto fail_cuda;
+    if (B.nind &&
+        (cudaMalloc(&rg->d_ind, sizeof(int64_t) * (size_t)B.nind) != cudaSuccess ||
+         cudaMemcpy(rg->d_ind, B.ind, sizeof(int64_t) * (size_t)B.nind, cudaMemcpyHostToDevice) != cudaSuccess))
+        goto fail_cuda;
     int64_t smem = 0;
-    for (int64_t i = 0; i < npass; i++)
+    for (int64_t i = 0; i < B.npass; i++)
     {
         unsigned char *base = (unsigned char *)pl->dtab;
-        const void **ptrs[7] = {&passes[i].tw, &passes[i].tw4_hi, &passes[i].tw4_lo, &passes[i].pre_tab,
-                                &passes[i].post_tab, &passes[i].mid_tab, &passes[i].rtw};
-        for (int t = 0; t < 7; t++) *ptrs[t] = toff[i][t] >= 0 ? base + toff[i][t] : NULL;
-        int64_t b = fftz_pass_smem_bytes(&passes[i]);
+        const void **ptrs[7] = {&B.passes[i].tw, &B.passes[i].tw4_hi, &B.passes[i].tw4_lo, &B.passes[i].pre_tab,
+                                &B.passes[i].post_tab, &B.passes[i].mid_tab, &B.passes[i].rtw};
+        for (int t = 0; t < 7; t++) *ptrs[t] = B.toff[i][t] >= 0 ? base + B.toff[i][t] : NULL;
+        if (B.indpos[i][0] >= 0) B.passes[i].ind_in = (const int64_t *)rg->d_ind + B.indpos[i][0];
+        if (B.indpos[i][1] >= 0) B.passes[i].ind_out = (const int64_t *)rg->d_ind + B.indpos[i][1];
+        int64_t b = fftz_pass_smem_bytes(&B.passes[i]);
         if (b > smem) smem = b;
     }
-    fftz_ritem_t *flat = (fftz_ritem_t *)malloc(sizeof(fftz_ritem_t) * (size_t)nitem);
+    flat = (fftz_ritem_t *)malloc(sizeof(fftz_ritem_t) * (size_t)B.nitem);
     if (!flat) goto fail_mem;
-    for (int64_t i = 0; i < nitem; i++) flat[i] = items[i].it;
-    int ok = cudaMalloc(&rg->d_passes, sizeof(fftz_pass_t) * (size_t)npass) == cudaSuccess &&
-             cudaMemcpy(rg->d_passes, passes, sizeof(fftz_pass_t) * (size_t)npass, cudaMemcpyHostToDevice) ==
+    for (int64_t i = 0; i < B.nitem; i++) flat[i] = B.items[i].it;
+    int ok = cudaMalloc(&rg->d_passes, sizeof(fftz_pass_t) * (size_t)B.npass) == cudaSuccess &&
+             cudaMemcpy(rg->d_passes, B.passes, sizeof(fftz_pass_t) * (size_t)B.npass, cudaMemcpyHostToDevice) ==
                  cudaSuccess &&
-             cudaMalloc(&rg->d_items, sizeof(fftz_ritem_t) * (size_t)nitem) == cudaSuccess &&
-             cudaMemcpy(rg->d_items, flat, sizeof(fftz_ritem_t) * (size_t)nitem, cudaMemcpyHostToDevice) ==
+             cudaMalloc(&rg->d_items, sizeof(fftz_ritem_t) * (size_t)B.nitem) == cudaSuccess &&
+             cudaMemcpy(rg->d_items, flat, sizeof(fftz_ritem_t) * (size_t)B.nitem, cudaMemcpyHostToDevice) ==
                  cudaSuccess &&
-             cudaMalloc(&rg->d_done, sizeof(int) * (size_t)npass) == cudaSuccess &&
+             cudaMalloc(&rg->d_done, sizeof(int) * (size_t)B.npass) == cudaSuccess &&
              cudaMalloc(&rg->d_queue, sizeof(unsigned long long)) == cudaSuccess &&
              cudaMalloc(&rg->d_err, sizeof(int)) == cudaSuccess &&
              cudaMemset(rg->d_err, 0, sizeof(int)) == cudaSuccess &&
-             (scratch_total == 0 || cudaMalloc(&pl->scratch, (size_t)scratch_total) == cudaSuccess) &&
+             (B.scratch_total == 0 || cudaMalloc(&pl->scratch, (size_t)B.scratch_total) == cudaSuccess) &&
              cudaStreamCreateWithFlags((cudaStream_t *)&rg->cap_stream, cudaStreamNonBlocking) == cudaSuccess;
-    free(flat);
     if (!ok) goto fail_cuda;
-    pl->scratch_bytes = scratch_total;
-    rg->npasses = npass;
-    rg->nitems = nitem;
+    pl->scratch_bytes = B.scratch_total;
+    rg->npasses = B.npass;
+    rg->nitems = B.nitem;
     rg->smem = (int)(smem < 1024 ? 1024 : smem);
     rg->grid = fftz_ragged_grid(dtype, rg->smem);
-    if (rg->grid > nitem) rg->grid = (int)nitem;
-    snprintf(rg->summary, sizeof(rg->summary), "ragged: %lld transforms, %lld passes, %lld tiles, grid %d x 256, %d B smem",
-             (long long)count, (long long)npass, (long long)nitem, rg->grid, rg->smem);
-    pl->in_bytes = rg->in_elems * csz;
-    pl->out_bytes = rg->out_elems * csz;
+    if (rg->grid > B.nitem) rg->grid = (int)B.nitem;
+    snprintf(rg->summary, sizeof(rg->summary),
+             "ragged: %lld transforms in %lld length groups, %lld passes, %lld tiles, grid %d x %d, %d B smem",
+             (long long)count, (long long)rg->ngroups, (long long)B.npass, (long long)B.nitem, rg->grid, RG_THREADS,
+             rg->smem);
+    pl->in_bytes = rg->in_elems * B.csz;
+    pl->out_bytes = rg->out_elems * B.csz;
     pl->nlaunch = 1;
-    free(passes);
-    free(toff);
-    free(items);
-    return pl;
+    goto done;
 fail_cuda:
     cudaGetLastError();
     fz_set_error("ragged setup: device allocation failed");
@@ -266,9 +435,6 @@ fail_cuda:
 fail_mem:
     fz_set_error("ragged setup: out of host memory");
 fail:
-    free(passes);
-    free(toff);
-    free(items);
     if (pl)
     {
         pl->rg = rg;
@@ -276,7 +442,20 @@ fail:
     }
     else
         free(rg);
-    return NULL;
+    pl = NULL;
+done:
+    free(flat);
+    free(B.passes);
+    free(B.toff);
+    free(B.indpos);
+    free(B.ind);
+    free(B.items);
+    free(ord);
+    free(tin);
+    free(tout);
+    free(gin);
+    free(gout);
+    return pl;
 }
 
 /* capture: reset counters, one launch of the executor */

@@ -37,6 +37,30 @@ template <typename T2> __device__ __forceinline__ T2 zero2() {
   return z;
 }
 
+// Input / output element offsets and column index of transform b of a pass
+// (col = index in bdim[0], -1 past the end). Batch dim ind_dim may be
+// indirect: its index then selects ind_in / ind_out entries.
+__device__ __forceinline__ void batch_offsets(const fftz_pass_t &P, int64_t b, int64_t *io_, int64_t *oo_,
+                                              int64_t *col_) {
+  int64_t io = 0, oo = 0, col = -1;
+  if (b < P.ntf) {
+    int64_t r = b;
+    col = 0;
+    for (int d = 0; d < P.nbdims; d++) {
+      const int64_t q = r / P.bdim[d];
+      const int64_t i = r - q * P.bdim[d];
+      if (d == 0) col = i;
+      const bool ind = d == P.ind_dim;
+      io += (ind && P.ind_in) ? P.ind_in[i] : i * P.ibs[d];
+      oo += (ind && P.ind_out) ? P.ind_out[i] : i * P.obs[d];
+      r = q;
+    }
+  }
+  *io_ = io;
+  *oo_ = oo;
+  *col_ = col;
+}
+
 // W_N^r for r = (col * k) mod N from two tables (factors formed in FP64, held
 // in the working precision): W = hi[r / L] * lo[r % L]. Powers of two take a
 // 32-bit path (r = col * k mod 2^32 reduced mod N is exact for N <= 2^31).

@@ -193,10 +193,23 @@ __device__ __forceinline__ void fast_stage(const fftz_pass_t &P, typename Cplx<T
             T2 *ob = (T2 *)P.out + s_out[p] + (int64_t)d0 * oes;
             const int64_t st = (int64_t)NS * oes;
             const bool cj = (P.flags & FFTZ_F_CONJ_OUT) != 0;
+            // four-step factor of output d0 + r NS: W^{col d0} (W^{col NS})^r,
+            // two table products per chain start and one for the step, then
+            // a chain of at most CH - 1 products (CH = 8 for radix 16)
+            constexpr int CH = R > 8 ? R / 2 : R;
+            T2 w = zero2<T2>(), stp = zero2<T2>();
+            if constexpr ((FEAT & FEAT_TW4) != 0) {
+              stp = tw4<T>(P, col, NS);
+              w = tw4<T>(P, col, d0);
+            }
 #pragma unroll
             for (int r = 0; r < R; r++) {
               T2 y = v[q][r];
-              if (FEAT & FEAT_TW4) y = cmul(y, tw4<T>(P, col, d0 + r * NS));
+              if constexpr ((FEAT & FEAT_TW4) != 0) {
+                if (r > 0 && r % CH == 0) w = tw4<T>(P, col, d0 + r * NS);
+                y = cmul(y, w);
+                if ((r + 1) % CH != 0) w = cmul(w, stp);
+              }
               if (cj) y.y = -y.y;
               ob[r * st] = y;
             }
@@ -239,36 +252,18 @@ struct FastStages<T, N, NST, NST, SW, NSW, FEAT, GLOBALIN> {
 // Base offsets and column index of the transforms of one tile.
 __device__ __forceinline__ void tile_offsets(const fftz_pass_t &P, int64_t tf0, int64_t *s_in, int64_t *s_out,
                                              int64_t *s_col) {
-  for (int p = threadIdx.x; p < P.tpc; p += blockDim.x) {
-    const int64_t b = tf0 + p;
-    int64_t io = 0, oo = 0, col = -1;
-    if (b < P.ntf) {
-      int64_t r = b;
-      col = 0;
-      for (int d = 0; d < P.nbdims; d++) {
-        const int64_t q = r / P.bdim[d];
-        const int64_t i = r - q * P.bdim[d];
-        if (d == 0) col = i;
-        io += i * P.ibs[d];
-        oo += i * P.obs[d];
-        r = q;
-      }
-    }
-    s_in[p] = io;
-    s_out[p] = oo;
-    s_col[p] = col;
-  }
+  for (int p = threadIdx.x; p < P.tpc; p += blockDim.x) batch_offsets(P, tf0 + p, s_in + p, s_out + p, s_col + p);
 }
 
+// One tile of a pass: transforms [tf0, tf0 + tpc) with blockDim == tpc * tpt.
 template <typename T, int N, int FEAT>
-__global__ void __launch_bounds__(ct_lb<T>()) fft_fast_kernel(const __grid_constant__ fftz_pass_t P) {
+__device__ __forceinline__ void fast_tile(const fftz_pass_t &P, int64_t tf0, unsigned char *smem_raw) {
   typedef typename Cplx<T>::type T2;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T2 *sdata = (T2 *)smem_raw;
   int64_t *s_in = (int64_t *)(sdata + (size_t)P.tpc * P.sstride);
   int64_t *s_out = s_in + P.tpc;
   int64_t *s_col = s_out + P.tpc;
-  tile_offsets(P, (int64_t)blockIdx.x * P.tpc, s_in, s_out, s_col);
+  tile_offsets(P, tf0, s_in, s_out, s_col);
   __syncthreads();
   if (FEAT & FEAT_SWEEP2) {
     constexpr int SH = Cplx<T>::PADSH;
@@ -287,6 +282,12 @@ __global__ void __launch_bounds__(ct_lb<T>()) fft_fast_kernel(const __grid_const
   } else {
     FastStages<T, N, 0, ct_nstages(N), 0, 1, FEAT, true>::run(P, sdata, s_in, s_out, s_col);
   }
+}
+
+template <typename T, int N, int FEAT>
+__global__ void __launch_bounds__(ct_lb<T>()) fft_fast_kernel(const __grid_constant__ fftz_pass_t P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fast_tile<T, N, FEAT>(P, (int64_t)blockIdx.x * P.tpc, smem_raw);
 }
 
 // ---------------------------------------------------------------- pipelined

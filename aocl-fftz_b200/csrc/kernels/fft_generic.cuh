@@ -287,25 +287,7 @@ __device__ __forceinline__ void generic_tile(const fftz_pass_t &P, int64_t blk, 
   int64_t *s_out = s_in + P.tpc;
   int64_t *s_col = s_out + P.tpc;
   const int64_t tf0 = blk * P.tpc;
-  for (int p = threadIdx.x; p < P.tpc; p += blockDim.x) {
-    const int64_t b = tf0 + p;
-    int64_t io = 0, oo = 0, col = -1;
-    if (b < P.ntf) {
-      int64_t r = b;
-      col = 0;
-      for (int d = 0; d < P.nbdims; d++) {
-        const int64_t q = r / P.bdim[d];
-        const int64_t i = r - q * P.bdim[d];
-        if (d == 0) col = i;
-        io += i * P.ibs[d];
-        oo += i * P.obs[d];
-        r = q;
-      }
-    }
-    s_in[p] = io;
-    s_out[p] = oo;
-    s_col[p] = col;
-  }
+  for (int p = threadIdx.x; p < P.tpc; p += blockDim.x) batch_offsets(P, tf0 + p, s_in + p, s_out + p, s_col + p);
   __syncthreads();
 
   const int nsweeps = (P.flags & FFTZ_F_MID_TAB) ? 2 : 1;

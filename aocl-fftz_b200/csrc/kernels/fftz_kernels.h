@@ -99,6 +99,12 @@ typedef struct fftz_pass
     const void *rtw;                    /* packed-real twiddles W_{2M}^k, working dtype */
     /* persistent executor only: in / out hold byte offsets into these bases */
     int32_t src_buf, dst_buf;           /* FFTZ_RBUF_* */
+    /* indirect batch dimension: when ind_in (ind_out) is set, index i of batch
+     * dim ind_dim contributes ind_in[i] (ind_out[i]) elements to the input
+     * (output) offset instead of i * ibs (i * obs) -- transforms of one length
+     * scattered through a packed ragged buffer form one batched pass */
+    int32_t ind_dim, pad_;
+    const int64_t *ind_in, *ind_out;
 } fftz_pass_t;
 
 /* Persistent DAG executor (fft_ragged.cu): one launch runs the CTA tiles of
@@ -114,6 +120,8 @@ typedef struct fftz_ritem
     int32_t dep;       /* pass that must complete first, -1 if none */
     int64_t blk;       /* CTA tile of the pass */
     int64_t dep_count; /* tiles of dep */
+    int32_t signal;    /* 1 if a later pass waits for this one: count the tile done */
+    int32_t pad_;
 } fftz_ritem_t;
 
 typedef struct fftz_ragged
@@ -133,6 +141,9 @@ typedef struct fftz_ragged
 } fftz_ragged_t;
 
 int fftz_launch_ragged(const fftz_ragged_t *r, int grid, void *stream);
+/* 1 if the executor has a compile-time tile for a pass of length n and
+ * FFTZ_VAR_FAST* variant (its tpc * tpt must then be 256). */
+int fftz_ragged_fast_ok(int n, int variant);
 /* CTAs of the persistent executor that fit on the device at once. */
 int fftz_ragged_grid(int dtype, int smem_bytes);
 

@@ -66,6 +66,26 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x, ws, device="cuda"):
+    """The largest value of x over all ranks (x itself on a single rank); every
+    rank must call it at the same point."""
+    if ws <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def step_metrics(n, batch_per_rank, esz, ws, ms):
+    """Whole-job 5N log2N GFLOP/s and algorithmic HBM GB/s of one fwd+bwd step
+    over ws ranks, each transforming batch_per_rank length-n lines, given the
+    step time in ms (the maximum over ranks)."""
+    flops = 2 * batch_per_rank * 5.0 * n * math.log2(n) * ws
+    alg_bytes = 2 * batch_per_rank * n * 2 * esz * ws  # each direction reads and writes the batch once
+    return flops / (ms * 1e-3) / 1e9, alg_bytes / (ms * 1e-3) / 1e9
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -226,15 +246,9 @@ def run_ours(args, wl):
     tb = (C.c_float * 16)()
     lib.aoclfftz_gpu_profile_end(pf, tf, 16)
     lib.aoclfftz_gpu_profile_end(pb, tb, 16)
-    if ws > 1:
-        t = torch.tensor([ms_total], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(ms_total, ws)
     ms = ms_total / K
-    flops_step = 2 * b * 5.0 * n * math.log2(n) * ws
-    value = flops_step / (ms * 1e-3) / 1e9
-    alg_bytes_step = 2 * b * n * 2 * esz * ws  # each direction reads and writes the batch once
-    hbm_gbs = alg_bytes_step / (ms * 1e-3) / 1e9
+    value, hbm_gbs = step_metrics(n, b, esz, ws, ms)
 
     # dominant kernel: the pass with the largest summed time
     passes = [("fwd",) + p for p in pass_table(lib, pf)] + [("bwd",) + p for p in pass_table(lib, pb)]
@@ -245,6 +259,7 @@ def run_ours(args, wl):
     peak, peak_kind = load_peaks()
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     res = dict(ms=ms, value=value, hbm_gbs=hbm_gbs, rt_err=rt_err, clocks=clk, launches=K * (npf + npb),
+               buffer_bytes=total * esz,
                roofline={"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": None,
                          "kernel": "%s %s" % (passes[dom][0], passes[dom][1]),
@@ -280,13 +295,10 @@ def run_ours(args, wl):
             estep()
         torch.cuda.synchronize()
         e_ms = (time.perf_counter() - t0) * 1e3 / KE
-        if ws > 1:
-            t = torch.tensor([e_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks(e_ms, ws)
         ez = hz.numpy().view(x.dtype)
         e_err = float(np.linalg.norm(ez / n - x) / np.linalg.norm(x))
-        res["e2e"] = {"value": round(flops_step / (e_ms * 1e-3) / 1e9, 2), "unit": "GFLOP/s",
+        res["e2e"] = {"value": round(step_metrics(n, b, esz, ws, e_ms)[0], 2), "unit": "GFLOP/s",
                       "h2d_bytes_per_step": 2 * b * n * esz, "d2h_bytes_per_step": 2 * b * n * esz,
                       "ms_per_step": round(e_ms, 3), "steps": KE, "round_trip_rel_l2": e_err,
                       "api": "aoclfftz_execute with pinned host in/out (library stages H2D, FFT, D2H)"}
@@ -400,6 +412,7 @@ def run_ragged(args, wl):
             "bytes_per_launch": per_launch, "ms_per_launch": round(ms / 2, 5),
             "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind}
     return dict(ms=ms, value=flops / (ms * 1e-3) / 1e9, hbm_gbs=alg_bytes / (ms * 1e-3) / 1e9, rt_err=rt,
+                buffer_bytes=total * esz,
                 clocks=clk, launches=2 * args.steps, roofline=roof,
                 extra={"plain_path": {"ms_per_step": round(ms_plain, 4),
                                       "value": round(flops / (ms_plain * 1e-3) / 1e9, 2),
@@ -585,7 +598,7 @@ def main():
             "vs_baseline": None, "dtype": wl["dtype"], "data": "synthetic (splitmix64 U[-1,1))",
             "config": {"workload": wl["desc"], "n": wl["n"], "batch_per_gpu": wl["batch"],
                        "global_batch": wl["batch"] * ws, "l2": "inputs larger than L2 (no flush needed)"
-                       if wl["n"] * wl["batch"] * 8 > 126e6 else "inputs fit L2",
+                       if r.get("buffer_bytes", 0) > 126e6 else "inputs fit L2 (no flush)",
                        "parallelism": "replicas dp%d" % ws},
             "hbm_gbs": round(r["hbm_gbs"], 1), "hbm_frac_of_measured": round(r["hbm_gbs"] / peak, 4),
             "gpu_launches": r["launches"], "clocks": r["clocks"], "round_trip_rel_l2": r["rt_err"]}

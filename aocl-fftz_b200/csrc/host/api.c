@@ -744,6 +744,16 @@ aoclfftz_error_type aoclfftz_gpu_synchronize(FFTZ_VOID *handle)
         fz_set_error("%s", cudaGetErrorString(e));
         return AOCLFFTZ_EXECUTION_FAILURE;
     }
+    for (int i = 0; i < pl->npass; i++)
+        if (!pl->pass[i].is_elem && pl->pass[i].k.use_tma)
+        {
+            if (fftz_tma_wait_failed())
+            {
+                fz_set_error("a TMA-fed pass gave up waiting for its tile copies (results invalid)");
+                return AOCLFFTZ_EXECUTION_FAILURE;
+            }
+            break;
+        }
     if (pl->rg && pl->rg->d_err)
     {
         int flag = 0;

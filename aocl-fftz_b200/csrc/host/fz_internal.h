@@ -128,6 +128,9 @@ int fz_tw4_tables(fz_blob *b, int dtype, int64_t N, int64_t *L, int64_t *off_hi,
 /* Bluestein tables for length n, pow2 convolution length m, direction */
 int fz_bluestein_tables(fz_blob *b, int dtype, int64_t n, int64_t m, int direction, int64_t *off_pre,
                         int64_t *off_post, int64_t *off_mid);
+/* appends the row-major copy T'[k1 * n2 + k2] = T[k1 + n1 * k2] of the table
+ * at off; returns its offset (-1 on allocation failure) */
+int64_t fz_blob_permute(fz_blob *b, int dtype, int64_t off, int64_t n1, int64_t n2);
 /* packed-real twiddles W_{2M}^k, k = 0..M (W^M = -1) */
 int64_t fz_real_twiddles(fz_blob *b, int dtype, int64_t M);
 

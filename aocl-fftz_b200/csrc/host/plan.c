@@ -15,7 +15,7 @@
  *           then row FFTs whose store performs the transpose)
  *   any prime factor > 13
  *       -> Bluestein over a power-of-two convolution length m >= 2n - 1, in one
- *          kernel when m fits shared memory, in four passes otherwise
+ *          kernel when m fits shared memory, in three passes otherwise
  *   N-D -> one line pass per dimension (dims[0] first, the rest in place)
  *   real, dims[0] even -> packed: n0/2-point complex FFT with the Hermitian
  *          recombination fused into the store (r2c) or the separation fused
@@ -252,6 +252,11 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
             k->variant = FFTZ_VAR_FAST_TW4;
         else
             k->variant = FFTZ_VAR_FAST;
+        /* TMA-fed tiles: by default for column passes (measured on B200: pass A
+         * of the 2^24 four-step 3% faster, row passes 13% slower), for every
+         * qualifying pass with kernel_family 5, never with kernel_family 1 */
+        k->use_tma = (k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4) &&
+                     (fam == 5 || (fam == 0 && k->in_mode == 1));
         if ((tw4 || tabs) && n < 32 && !(variant_bits & 4))
         {
             /* small feature kernels are not instantiated: use the generic one */
@@ -506,7 +511,9 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
                  (long long)p->k.ntf);
         return 0;
     }
-    /* four passes: FFT_m(pad(x c)) * conj... through S0/S1 */
+    /* three passes through S0 / S1: A (column FFTs of the chirped, padded
+     * input), M (row FFTs, spectrum product, row FFTs of the second FFT_m),
+     * D (row FFTs of the second FFT_m, output chirp) */
     int64_t n1, n2;
     if (choose_split(pl, m, &n1, &n2)) return -1;
     int64_t lines = lines_of(b, nb);
@@ -538,7 +545,14 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
     pa->off_tw4hi = hi;
     pa->off_tw4lo = lo;
     pa->off_pre = pre;
-    /* B: S0 -> S1, row FFTs, store conj(A) * conj(Bhat) in natural order */
+    /* M: S0 -> S1, one pass per row k1 (contiguous j2): forward FFT over j2
+     * (the second half of FFT_m of the chirped input, spectrum index
+     * k = k1 + n1 k2), v = conj(v) * conj(Bhat)[k] (table rows made contiguous),
+     * then the first half of the second FFT_m with the split swapped
+     * (n2 x n1): the FFT over k2 for this k1, times W_m^{k1 k1'}, stored
+     * transposed as S1[k1'][k1]. Three passes through scratch instead of four. */
+    const int64_t midT = fz_blob_permute(&pl->blob, pl->dtype, mid, n1, n2);
+    if (midT < 0) return -1;
     bb[0].n = n1;
     bb[0].is = n2;
     bb[0].os = 1;
@@ -550,32 +564,20 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
         bb[i + 1].os = so;
         so *= b[i].n;
     }
-    fz_pass *pb = line_pass(pl, n2, 1, n1, bb, nb + 1, 1, S0, S1, FFTZ_F_CONJ_OUT | FFTZ_F_POST_TAB, 2);
-    if (!pb) return -1;
-    pb->k.post_es = n1;
-    pb->k.post_cs = 1;
-    pb->off_post = mid;
-    /* C: S1 -> S0, column FFTs with the four-step twiddle */
+    fz_pass *pm = line_pass(pl, n2, 1, n1, bb, nb + 1, 1, S0, S1, FFTZ_F_MID_TAB | FFTZ_F_TW4, 2 | 4);
+    if (!pm) return -1;
+    pm->k.mid_cs = n2;
+    pm->off_mid = midT;
+    pm->k.tw4_n = m;
+    pm->k.tw4_l = L;
+    pm->off_tw4hi = hi;
+    pm->off_tw4lo = lo;
+    snprintf(pm->what, sizeof(pm->what), "bluestein-mid n=%lld m=%lld x%lld", (long long)n, (long long)m,
+             (long long)pm->k.ntf);
+    /* D: S1 -> dst, rows k1' (contiguous k1): FFT over k1 -> k2', output
+     * k' = k1' + n2 k2' in natural order, X_k' = chirp_k' * conv_k' / m for k' < n */
     bb[0].n = n2;
-    bb[0].is = 1;
-    bb[0].os = 1;
-    so = m;
-    for (int i = 0; i < nb; i++)
-    {
-        bb[i + 1] = b[i];
-        bb[i + 1].is = so;
-        bb[i + 1].os = so;
-        so *= b[i].n;
-    }
-    fz_pass *pc = line_pass(pl, n1, n2, n2, bb, nb + 1, 1, S1, S0, FFTZ_F_TW4, 0);
-    if (!pc) return -1;
-    pc->k.tw4_n = m;
-    pc->k.tw4_l = L;
-    pc->off_tw4hi = hi;
-    pc->off_tw4lo = lo;
-    /* D: S0 -> dst, row FFTs, X_k = chirp_k * conv_k / m for k < n */
-    bb[0].n = n1;
-    bb[0].is = n2;
+    bb[0].is = n1;
     bb[0].os = oes;
     so = m;
     for (int i = 0; i < nb; i++)
@@ -584,11 +586,11 @@ static int bluestein(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, const fz_
         bb[i + 1].is = so;
         so *= b[i].n;
     }
-    fz_pass *pd = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, S0, dst,
+    fz_pass *pd = line_pass(pl, n1, 1, n2 * oes, bb, nb + 1, 1, S1, dst,
                             (bwd ? 0 : FFTZ_F_CONJ_OUT) | FFTZ_F_POST_TAB, 2);
     if (!pd) return -1;
     pd->k.post_n = n;
-    pd->k.post_es = n1;
+    pd->k.post_es = n2;
     pd->k.post_cs = 1;
     pd->off_post = post;
     return 0;

@@ -255,3 +255,16 @@ int64_t fz_real_twiddles(fz_blob *b, int dtype, int64_t M)
     put_c(b, off, dtype, M, -1.0, 0.0);
     return off;
 }
+
+int64_t fz_blob_permute(fz_blob *b, int dtype, int64_t off, int64_t n1, int64_t n2)
+{
+    /* T'[k1 * n2 + k2] = T[k1 + n1 * k2]: the rows of an n1 x n2 table become
+     * contiguous (a table read along k2 for a fixed k1) */
+    const size_t esz = dtype == 0 ? 8 : 16;
+    int64_t o = fz_blob_reserve(b, (size_t)(n1 * n2) * esz);
+    if (o < 0) return -1;
+    for (int64_t k1 = 0; k1 < n1; k1++)
+        for (int64_t k2 = 0; k2 < n2; k2++)
+            memcpy(b->p + o + (size_t)(k1 * n2 + k2) * esz, b->p + off + (size_t)(k1 + n1 * k2) * esz, esz);
+    return o;
+}

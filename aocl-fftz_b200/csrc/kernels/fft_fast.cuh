@@ -96,10 +96,16 @@ __device__ __forceinline__ typename Cplx<T>::type load_fast(const fftz_pass_t &P
 
 // One Stockham stage. FROMG: the stage reads its inputs from HBM (otherwise
 // from shared memory). LAST: it writes its outputs to HBM. MAPFIRST /
-// MAPLAST select the HBM-side lane map (in_mode / out_mode).
-template <typename T, int N, int S, int FEAT, bool FROMG, bool LAST, bool MAPFIRST, bool CONJ0 = false>
+// MAPLAST select the HBM-side lane map (in_mode / out_mode). STG: the first
+// stage's inputs were staged densely in sdata by the tensor-memory
+// accelerator (transform p at s_in[p], element e at e * stg_es); the stage
+// reads them with the HBM lane map and waits for every thread before it
+// overwrites the staging area with its own outputs.
+template <typename T, int N, int S, int FEAT, bool FROMG, bool LAST, bool MAPFIRST, bool CONJ0 = false,
+          bool STG = false>
 __device__ __forceinline__ void fast_stage(const fftz_pass_t &P, typename Cplx<T>::type *sdata,
-                                           const int64_t *s_in, const int64_t *s_out, const int64_t *s_col) {
+                                           const int64_t *s_in, const int64_t *s_out, const int64_t *s_col,
+                                           int stg_es = 1) {
   typedef typename Cplx<T>::type T2;
   constexpr int R = ct_radix(N, S);
   constexpr int NS = ct_ns(N, S);
@@ -123,7 +129,25 @@ __device__ __forceinline__ void fast_stage(const fftz_pass_t &P, typename Cplx<T
   const int64_t col = s_col[p];
   const bool valid = col >= 0;
   T2 v[NB][R];
-  if (FROMG) {
+  if (FROMG && STG) {
+    const T2 *src = sdata + s_in[p];
+    const bool cj = (P.flags & FFTZ_F_CONJ_IN) != 0;
+#pragma unroll
+    for (int q = 0; q < NB; q++) {
+      const int b = j + q * TPT;
+      if (ALLV || b < NBF) {
+        const T2 *sb = src + b * stg_es;
+        const int st = NBF * stg_es;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          T2 x = sb[r * st];
+          if (cj) x.y = -x.y;
+          v[q][r] = x;
+        }
+      }
+    }
+    __syncthreads();
+  } else if (FROMG) {
     const T2 *gin = (const T2 *)P.in + s_in[p];
 #pragma unroll
     for (int q = 0; q < NB; q++) {
@@ -234,19 +258,21 @@ __device__ __forceinline__ void fast_stage(const fftz_pass_t &P, typename Cplx<T
 
 // Stage S of sweep SW out of NSW sweeps. GLOBALIN: the very first stage reads
 // HBM (fast kernel); the pipelined kernel has already staged the tile.
-template <typename T, int N, int S, int NST, int SW, int NSW, int FEAT, bool GLOBALIN> struct FastStages {
+template <typename T, int N, int S, int NST, int SW, int NSW, int FEAT, bool GLOBALIN, bool STG = false>
+struct FastStages {
   static __device__ __forceinline__ void run(const fftz_pass_t &P, typename Cplx<T>::type *sdata,
-                                             const int64_t *s_in, const int64_t *s_out, const int64_t *s_col) {
+                                             const int64_t *s_in, const int64_t *s_out, const int64_t *s_col,
+                                             int stg_es = 1) {
     constexpr bool FIRSTG = (S == 0 && SW == 0);
     fast_stage<T, N, S, FEAT, GLOBALIN && FIRSTG, (S == NST - 1 && SW == NSW - 1), GLOBALIN && FIRSTG,
-               !GLOBALIN && FIRSTG>(P, sdata, s_in, s_out, s_col);
-    FastStages<T, N, S + 1, NST, SW, NSW, FEAT, GLOBALIN>::run(P, sdata, s_in, s_out, s_col);
+               !GLOBALIN && FIRSTG, STG && FIRSTG>(P, sdata, s_in, s_out, s_col, stg_es);
+    FastStages<T, N, S + 1, NST, SW, NSW, FEAT, GLOBALIN, STG>::run(P, sdata, s_in, s_out, s_col, stg_es);
   }
 };
-template <typename T, int N, int NST, int SW, int NSW, int FEAT, bool GLOBALIN>
-struct FastStages<T, N, NST, NST, SW, NSW, FEAT, GLOBALIN> {
+template <typename T, int N, int NST, int SW, int NSW, int FEAT, bool GLOBALIN, bool STG>
+struct FastStages<T, N, NST, NST, SW, NSW, FEAT, GLOBALIN, STG> {
   static __device__ __forceinline__ void run(const fftz_pass_t &, typename Cplx<T>::type *, const int64_t *,
-                                             const int64_t *, const int64_t *) {}
+                                             const int64_t *, const int64_t *, int = 1) {}
 };
 
 // Base offsets and column index of the transforms of one tile.
@@ -272,10 +298,12 @@ __device__ __forceinline__ void fast_tile(const fftz_pass_t &P, int64_t tf0, uns
     for (int i = threadIdx.x; i < P.tpc * N; i += blockDim.x) {
       const int p = i / N;
       const int e = i - p * N;
+      const int64_t c = s_col[p];
+      if (c < 0) continue;
       T2 *a = sdata + (size_t)p * P.sstride + phys<SH>(e);
       T2 v = *a;
       v.y = -v.y;
-      *a = cmul(v, __ldg(mt + e));
+      *a = cmul(v, __ldg(mt + e + c * P.mid_cs));
     }
     __syncthreads();
     FastStages<T, N, 0, ct_nstages(N), 1, 2, FEAT, true>::run(P, sdata, s_in, s_out, s_col);

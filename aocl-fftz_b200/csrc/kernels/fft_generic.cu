@@ -87,6 +87,10 @@ int64_t fftz_pass_smem_bytes(const fftz_pass_t *p) {
 }
 
 int fftz_launch_pass(const fftz_pass_t *p, void *stream) {
+  if (p->use_tma) {
+    const int e = fftz_launch_pass_tma(p, stream);
+    if (e >= 0) return e;
+  }
   // one opt-in of the large dynamic shared memory size per kernel and device
   static const void *opted[64][96];
   static int nopted[64];

@@ -307,10 +307,12 @@ __device__ __forceinline__ void generic_tile(const fftz_pass_t &P, int64_t blk, 
       for (int i = threadIdx.x; i < P.tpc * P.n; i += blockDim.x) {
         const int p = i / P.n;
         const int e = i - p * P.n;
+        const int64_t c = s_col[p];
+        if (c < 0) continue;
         T2 *a = sdata + (size_t)p * P.sstride + phys<SH>(e);
         T2 v = *a;
         v.y = -v.y;
-        *a = cmul(v, __ldg(mt + e));
+        *a = cmul(v, __ldg(mt + e + c * P.mid_cs));
       }
       __syncthreads();
     }

@@ -52,7 +52,7 @@ __device__ __forceinline__ bool ragged_fast(const fftz_pass_t &P, int64_t blk, u
   } else if (P.variant == FFTZ_VAR_FAST_TW4) {
     switch (P.n) { FZ_RG_CASE(64, 1) FZ_RG_CASE(128, 1) FZ_RG_CASE(256, 1) FZ_RG_CASE(512, 1) }
   } else if (P.variant == FFTZ_VAR_FAST_TABS) {
-    switch (P.n) { FZ_RG_CASE(64, 2) FZ_RG_CASE(128, 2) FZ_RG_CASE(256, 2) }
+    switch (P.n) { FZ_RG_CASE(64, 2) FZ_RG_CASE(128, 2) FZ_RG_CASE(256, 2) FZ_RG_CASE(512, 2) }
   } else if (P.variant == FFTZ_VAR_FAST_TW4_TABS) {
     switch (P.n) { FZ_RG_CASE(128, 3) FZ_RG_CASE(256, 3) FZ_RG_CASE(512, 3) }
   } else if (P.variant == FFTZ_VAR_FAST_BLUE) {
@@ -122,7 +122,7 @@ extern "C" int fftz_ragged_fast_ok(int n, int variant) {
   const bool p2 = n >= 2 && n <= 4096 && (n & (n - 1)) == 0;
   if (variant == FFTZ_VAR_FAST) return p2;
   if (variant == FFTZ_VAR_FAST_TW4) return p2 && n >= 64 && n <= 512;
-  if (variant == FFTZ_VAR_FAST_TABS) return p2 && n >= 64 && n <= 256;
+  if (variant == FFTZ_VAR_FAST_TABS) return p2 && n >= 64 && n <= 512;
   if (variant == FFTZ_VAR_FAST_TW4_TABS) return p2 && n >= 128 && n <= 512;
   if (variant == FFTZ_VAR_FAST_BLUE) return p2 && n >= 4;
   return 0;

@@ -1,0 +1,250 @@
+// Tensor-memory-accelerator (TMA) input path of the compile-time FFT kernel.
+//
+// The one-tile-per-CTA kernel of fft_fast.cuh fetches its tile with ordinary
+// per-thread loads fused into the first stage. Column passes (lanes along
+// neighbouring transforms) read only tpc * element-size contiguous bytes per
+// row, so the load path issues many narrow requests. Here one thread issues
+// cp.async.bulk.tensor copies of the whole tile -- boxes of (tpc columns x 256
+// rows) for column passes, (256 elements x 1 row) for row passes -- into the
+// shared-memory tile, completion is tracked by an mbarrier transaction count,
+// and the first stage reads the dense staged tile instead of HBM (the stage
+// code is the same template with its STG flag). Stores are unchanged.
+//
+// Eligibility is decided per launch on the host (the tensor map encodes the
+// buffer address): complex input, plain or four-step-twiddle variant, at most
+// two batch dimensions, tiles that do not straddle the outer batch dimension,
+// 16-byte aligned base and strides. Anything else takes the ordinary kernel.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_fast.cuh"
+
+namespace fftz {
+
+__device__ int g_tma_wait_failed;  // set when a tile's copies did not arrive in time
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_addr(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// One tile per CTA. MODE 1: column pass (tile = tpc adjacent columns, staged
+// [e][p]); MODE 0: row pass (tile = tpc rows, staged [p][e]).
+template <typename T, int N, int FEAT, int MODE>
+__global__ void __launch_bounds__(ct_lb<T>()) fft_tma_kernel(const __grid_constant__ fftz_pass_t P,
+                                                            const __grid_constant__ CUtensorMap tmap) {
+  typedef typename Cplx<T>::type T2;
+  constexpr int BOXE = N < 256 ? N : 256;   // elements of one box along the transform
+  constexpr int CE = sizeof(T2) / 8;        // 8-byte units per complex element
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  // 128-byte aligned tile (the host adds 128 bytes of slack)
+  unsigned char *base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+  T2 *sdata = (T2 *)base;
+  int64_t *s_in = (int64_t *)(sdata + (size_t)P.tpc * P.sstride);
+  int64_t *s_out = s_in + P.tpc;
+  int64_t *s_col = s_out + P.tpc;
+  const int64_t tf0 = (int64_t)blockIdx.x * P.tpc;
+  const int tpc = P.tpc;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&bar, (unsigned)(N * tpc * sizeof(T2)));
+    const int64_t b0 = P.bdim[0];
+    const int c0 = (int)(tf0 % b0);
+    const int z = (int)(tf0 / b0);
+    if (MODE == 1) {
+      for (int k = 0; k < N / BOXE; k++)
+        tma_load_3d(sdata + (size_t)k * BOXE * tpc, &tmap, c0 * CE, k * BOXE, z, &bar);
+    } else {
+      for (int q = 0; q < tpc; q++)
+        for (int k = 0; k < N / BOXE; k++) tma_load_3d(sdata + (size_t)q * N + k * BOXE, &tmap, k * BOXE * CE, c0 + q, z, &bar);
+    }
+  }
+  for (int p = threadIdx.x; p < tpc; p += blockDim.x) {
+    int64_t io;
+    batch_offsets(P, tf0 + p, &io, s_out + p, s_col + p);
+    s_in[p] = MODE == 1 ? p : (int64_t)p * N;
+  }
+  // bounded wait for the tile (about a second of polling); a wait that gives
+  // up leaves the tile unwritten and flags the failure for the host
+  bool ok = false;
+  for (long i = 0; i < (1L << 22); i++)
+    if (mbar_try_wait(&bar, 0)) {
+      ok = true;
+      break;
+    }
+  if (!__syncthreads_and(ok)) {  // every thread takes the same branch
+    if (threadIdx.x == 0) atomicExch(&g_tma_wait_failed, 1);
+    return;
+  }
+  FastStages<T, N, 0, ct_nstages(N), 0, 1, FEAT, true, true>::run(P, sdata, s_in, s_out, s_col,
+                                                                   MODE == 1 ? tpc : 1);
+}
+
+}  // namespace fftz
+
+// ------------------------------------------------------------------- host
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+int g_encode_state = 0;  // 0 unknown, 1 ready, -1 unavailable
+
+bool encoder() {
+  if (g_encode_state == 0) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && fn) {
+      g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+      g_encode_state = 1;
+    } else {
+      cudaGetLastError();
+      g_encode_state = -1;
+    }
+  }
+  return g_encode_state == 1;
+}
+
+template <typename T, int FEAT, int MODE>
+const void *pick(int n) {
+  switch (n) {
+    case 256: return (const void *)&fftz::fft_tma_kernel<T, 256, FEAT, MODE>;
+    case 512: return (const void *)&fftz::fft_tma_kernel<T, 512, FEAT, MODE>;
+    case 1024: return (const void *)&fftz::fft_tma_kernel<T, 1024, FEAT, MODE>;
+    case 2048: return (const void *)&fftz::fft_tma_kernel<T, 2048, FEAT, MODE>;
+    case 4096: return (const void *)&fftz::fft_tma_kernel<T, 4096, FEAT, MODE>;
+  }
+  return nullptr;
+}
+
+const void *tma_kernel(int dtype, int n, int tw4, int mode) {
+  if (dtype == 0)
+    return tw4 ? (mode ? pick<float, 1, 1>(n) : pick<float, 1, 0>(n))
+               : (mode ? pick<float, 0, 1>(n) : pick<float, 0, 0>(n));
+  return tw4 ? (mode ? pick<double, 1, 1>(n) : pick<double, 1, 0>(n))
+             : (mode ? pick<double, 0, 1>(n) : pick<double, 0, 0>(n));
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Launches pass p through the TMA kernel. Returns -1 (nothing launched) when
+ * the pass or its buffers do not qualify, else a cudaError_t value. */
+int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
+  if (p->variant != FFTZ_VAR_FAST && p->variant != FFTZ_VAR_FAST_TW4) return -1;
+  if (p->in_kind != FFTZ_IN_COMPLEX || p->nbdims < 1 || p->nbdims > 2 || p->ind_in) return -1;
+  const int mode = p->in_mode;
+  const int64_t esz = p->dtype == 0 ? 8 : 16, ce = esz / 8;
+  const int64_t b0 = p->bdim[0], b1 = p->nbdims == 2 ? p->bdim[1] : 1;
+  if (p->tpc < 1 || b0 % p->tpc || p->ntf != b0 * b1) return -1;
+  if (((uintptr_t)p->in & 15) != 0) return -1;
+  const void *fn = tma_kernel(p->dtype, p->n, p->variant == FFTZ_VAR_FAST_TW4, mode);
+  if (!fn || !encoder()) return -1;
+  const int64_t n = p->n, boxe = n < 256 ? n : 256;
+  cuuint64_t dims[3], strides[2];
+  cuuint32_t box[3], estr[3] = {1, 1, 1};
+  if (mode == 1) {
+    /* columns: element e at e * ies, column c at c (contiguous), outer batch at ibs[1] */
+    if (p->ibs[0] != 1 || (p->tpc * esz) % 16) return -1;
+    dims[0] = (cuuint64_t)(b0 * ce);
+    dims[1] = (cuuint64_t)n;
+    strides[0] = (cuuint64_t)(p->ies * esz);
+    box[0] = (cuuint32_t)(p->tpc * ce);
+    box[1] = (cuuint32_t)boxe;
+  } else {
+    /* rows: element e contiguous, row r at ibs[0] */
+    if (p->ies != 1) return -1;
+    dims[0] = (cuuint64_t)(n * ce);
+    dims[1] = (cuuint64_t)b0;
+    strides[0] = (cuuint64_t)(p->ibs[0] * esz);
+    box[0] = (cuuint32_t)(boxe * ce);
+    box[1] = 1;
+  }
+  dims[2] = (cuuint64_t)b1;
+  strides[1] = p->nbdims == 2 ? (cuuint64_t)(p->ibs[1] * esz) : (cuuint64_t)((strides[0] * dims[1] + 15) & ~15ULL);
+  box[2] = 1;
+  if (strides[0] % 16 || strides[1] % 16 || strides[0] >= (1ULL << 40) || strides[1] >= (1ULL << 40)) return -1;
+  CUtensorMap map;
+  if (g_encode(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, (void *)p->in, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return -1;
+  static const void *opted[64][64];
+  static int nopted[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  static int maxdyn[64][64];
+  const size_t smem = (size_t)fftz_pass_smem_bytes(p) + 128;
+  int slot = -1;
+  for (int i = 0; i < nopted[dev]; i++)
+    if (opted[dev][i] == fn) slot = i;
+  if (slot < 0) {
+    /* the kernel's static shared memory (its mbarrier) counts against the limit */
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) return (int)cudaGetLastError();
+    const int md = (int)(fftz_smem_limit() - (int64_t)fa.sharedSizeBytes);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+    if (e != cudaSuccess) return (int)e;
+    if (nopted[dev] < 64) {
+      slot = nopted[dev]++;
+      opted[dev][slot] = fn;
+      maxdyn[dev][slot] = md;
+    }
+  }
+  if (slot < 0 || smem > (size_t)maxdyn[dev][slot]) return -1;
+  const dim3 block((unsigned)(p->tpc * p->tpt));
+  const dim3 grid((unsigned)(p->ntf / p->tpc));
+  void *args[2] = {(void *)p, (void *)&map};
+  return (int)cudaLaunchKernel(fn, grid, block, args, smem, (cudaStream_t)stream);
+}
+
+/* 1 if some TMA tile gave up waiting for its copies since the last call (and
+ * clears the flag); 0 otherwise. */
+int fftz_tma_wait_failed(void) {
+  int v = 0, z = 0;
+  if (cudaMemcpyFromSymbol(&v, fftz::g_tma_wait_failed, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (v) cudaMemcpyToSymbol(fftz::g_tma_wait_failed, &z, sizeof(int));
+  return v;
+}
+
+}  // extern "C"

@@ -90,6 +90,7 @@ typedef struct fftz_pass
     int64_t tw4_n, tw4_l;               /* W_{tw4_n}^r = hi[r / tw4_l] * lo[r % tw4_l] */
     int64_t pre_n, pre_es, pre_cs;      /* load bound (0: none) and table index map */
     int64_t post_n, post_es, post_cs;   /* store bound (0: none) and table index map */
+    int64_t mid_cs;                     /* mid_tab index of element e of column col: e + col * mid_cs */
     double scale;
     const void *in;
     void *out;
@@ -103,7 +104,8 @@ typedef struct fftz_pass
      * dim ind_dim contributes ind_in[i] (ind_out[i]) elements to the input
      * (output) offset instead of i * ibs (i * obs) -- transforms of one length
      * scattered through a packed ragged buffer form one batched pass */
-    int32_t ind_dim, pad_;
+    int32_t ind_dim;
+    int32_t use_tma;                    /* fetch the tile with TMA copies when the pass qualifies */
     const int64_t *ind_in, *ind_out;
 } fftz_pass_t;
 
@@ -205,6 +207,11 @@ int64_t fftz_smem_limit(void);
 
 /* Launches one pass on the given stream; returns a cudaError_t value. */
 int fftz_launch_pass(const fftz_pass_t *p, void *stream);
+/* The TMA-fed variant of a compile-time pass (fft_tma.cu): -1 when the pass
+ * or its buffers do not qualify (nothing launched), else a cudaError_t. */
+int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream);
+/* 1 if a TMA tile gave up waiting for its copies since the last call. */
+int fftz_tma_wait_failed(void);
 
 #ifdef __cplusplus
 }

@@ -107,8 +107,10 @@ CANDIDATES = [
     dict(),                                   # the planner's default
     dict(tpc_row=1), dict(tpc_row=2), dict(tpc_row=4),
     dict(tpc_col=2), dict(tpc_col=4), dict(tpc_col=8), dict(tpc_col=16),
+    dict(kernel_family=1),                    # plain loads everywhere (no TMA-fed column passes)
     dict(kernel_family=2),
     dict(kernel_family=3),                    # generic kernel only
+    dict(kernel_family=5),                    # TMA-fed tiles wherever they qualify
     dict(fourstep_n1=256), dict(fourstep_n1=1024), dict(fourstep_n1=4096),
     dict(algorithm=2),                        # force a four-step split where possible
 ]

@@ -55,7 +55,10 @@ FFTZ_INT32 aoclfftz_gpu_pass_info(FFTZ_VOID *handle, FFTZ_INT32 i, FFTZ_CHAR *bu
  *   batch_chunk   multi-pass plans run their passes on chunks of this many
  *                 lines at a time (keeps the intermediate resident in L2)
  *   algorithm     1 one pass, 2 four-step, 3 Bluestein (0 = choose)
- *   kernel_family 1 one tile per CTA, 2 persistent double-buffered (0 = choose)
+ *   kernel_family 1 one tile per CTA, loads by the threads; 2 persistent
+ *                 double-buffered; 3 generic kernel only; 5 one tile per CTA
+ *                 fetched by TMA copies wherever the pass qualifies
+ *                 (0 = choose: TMA copies for column passes)
  * aoclfftz_gpu_set_hints(NULL) restores the defaults. */
 typedef struct aoclfftz_gpu_hints
 {

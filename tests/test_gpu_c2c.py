@@ -8,6 +8,8 @@ Cases follow the reference's test design: every radix and the pow2 iterative,
 four-step, Cooley-Tukey and Bluestein paths (test/bench/CMakeLists.txt:55-124),
 strided and batched layouts, in- and out-of-place, both directions.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -158,3 +160,25 @@ def test_bit_reproducible():
     outs, _ = run_gpu("f64", [(65521, 1, 1)], [(4, 65521, 65521)], x, 2 * 4 * 65521, repeat=3)
     for o in outs[1:]:
         assert o.tobytes() == outs[0].tobytes()
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n,batch", [(1 << 16, 3), (1 << 20, 2), (1 << 24, 1), (4096, 64), (1024, 40)])
+def test_tma_fed_passes(dtype, n, batch):
+    """Kernel family 5 (tiles fetched by TMA copies) against the oracle, both
+    directions; the four-step passes qualify for column and row TMA boxes."""
+    if dtype == "f64" and n == 1 << 24:
+        n = 1 << 22
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi
+    lib = aoclfftz_b200.load()
+    h = abi.Hints()
+    h.kernel_family = 5
+    lib.aoclfftz_gpu_set_hints(C.byref(h))
+    try:
+        for d in (0, 1):
+            if n >= 1 << 20:
+                check_c2c(dtype, [(n, 1, 1)], [(batch, n, n)], d, compare_ref=False)
+            else:
+                check_c2c(dtype, [(n, 1, 1)], [(batch, n, n)], d)
+    finally:
+        lib.aoclfftz_gpu_set_hints(None)

@@ -256,7 +256,10 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
          * of the 2^24 four-step 3% faster, row passes 13% slower), for every
          * qualifying pass with kernel_family 5, never with kernel_family 1 */
         k->use_tma = (k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4) &&
-                     (fam == 5 || (fam == 0 && k->in_mode == 1));
+                     (fam == 5 || fam == 6 || (fam == 0 && k->in_mode == 1));
+        if (k->use_tma && fam == 6) k->use_tma = 2; /* persistent, next tile half-prefetched */
+        /* stage twiddles copied to shared memory by each CTA (hint twiddles = 2) */
+        k->smem_tw = pl->hints.twiddles == 2 && !ragged_mode(pl) && n >= 512;
         if ((tw4 || tabs) && n < 32 && !(variant_bits & 4))
         {
             /* small feature kernels are not instantiated: use the generic one */
@@ -296,6 +299,7 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         maxthr = fast_max_threads(pl);
         finish_launch_shape(pl, k, nslots, maxthr);
     }
+    if (k->smem_tw && fftz_pass_smem_bytes(k) > fftz_smem_limit()) k->smem_tw = 0;
     if (fftz_pass_smem_bytes(k) > fftz_smem_limit())
     {
         fz_set_error("length %lld does not fit shared memory", (long long)n);

@@ -45,6 +45,16 @@ __host__ __device__ constexpr int ct_ns(int n, int s) {
   return p;
 }
 __host__ __device__ constexpr int ct_tpt(int n) { return n >= 16 ? n / 16 : 1; }
+// Entries of the stage-twiddle table (entry 0 unused, stage s >= 1 holds
+// (R_s - 1) * Ns entries).
+__host__ __device__ constexpr int ct_tw_total(int n) {
+  int t = 1, ns = 1;
+  for (int s = 0; s < ct_nstages(n); s++) {
+    if (s > 0) t += (ct_radix(n, s) - 1) * ns;
+    ns *= ct_radix(n, s);
+  }
+  return t;
+}
 // Block-size bound of an instantiation: room for several columns per CTA
 // (1024 threads for float, 512 for double keeps the double kernels at <= 128
 // registers).
@@ -101,11 +111,15 @@ __device__ __forceinline__ typename Cplx<T>::type load_fast(const fftz_pass_t &P
 // accelerator (transform p at s_in[p], element e at e * stg_es); the stage
 // reads them with the HBM lane map and waits for every thread before it
 // overwrites the staging area with its own outputs.
+// STG == 2: the half e < N/2 of every transform was staged in stg (transform
+// p at stg_off[p], element e at e * stg_es); the other half is read from HBM.
 template <typename T, int N, int S, int FEAT, bool FROMG, bool LAST, bool MAPFIRST, bool CONJ0 = false,
-          bool STG = false>
+          int STG = 0>
 __device__ __forceinline__ void fast_stage(const fftz_pass_t &P, typename Cplx<T>::type *sdata,
                                            const int64_t *s_in, const int64_t *s_out, const int64_t *s_col,
-                                           int stg_es = 1) {
+                                           int stg_es = 1, const typename Cplx<T>::type *stg = nullptr,
+                                           const int64_t *stg_off = nullptr,
+                                           const typename Cplx<T>::type *twb = nullptr) {
   typedef typename Cplx<T>::type T2;
   constexpr int R = ct_radix(N, S);
   constexpr int NS = ct_ns(N, S);
@@ -129,7 +143,28 @@ __device__ __forceinline__ void fast_stage(const fftz_pass_t &P, typename Cplx<T
   const int64_t col = s_col[p];
   const bool valid = col >= 0;
   T2 v[NB][R];
-  if (FROMG && STG) {
+  if (FROMG && STG == 2) {
+    const T2 *gin = (const T2 *)P.in + s_in[p];
+    const T2 *src = stg + stg_off[p];
+    const bool cj = (P.flags & FFTZ_F_CONJ_IN) != 0;
+    const int64_t ies = P.ies;
+#pragma unroll
+    for (int q = 0; q < NB; q++) {
+      const int b = j + q * TPT;
+      if (ALLV || b < NBF) {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          T2 x = zero2<T2>();
+          if (r < R / 2)
+            x = src[(b + r * NBF) * stg_es];  // e < N/2: staged
+          else if (valid)
+            x = gin[(int64_t)(b + r * NBF) * ies];
+          if (cj) x.y = -x.y;
+          v[q][r] = x;
+        }
+      }
+    }
+  } else if (FROMG && STG) {
     const T2 *src = sdata + s_in[p];
     const bool cj = (P.flags & FFTZ_F_CONJ_IN) != 0;
 #pragma unroll
@@ -195,15 +230,21 @@ __device__ __forceinline__ void fast_stage(const fftz_pass_t &P, typename Cplx<T
     }
     __syncthreads();
   }
-  const T2 *tw = (const T2 *)P.tw + P.tw_off[S];
+  // stage twiddles from the shared-memory copy when the tile made one
+  const T2 *tw = (twb ? twb : (const T2 *)P.tw) + P.tw_off[S];
 #pragma unroll
   for (int q = 0; q < NB; q++) {
     const int b = j + q * TPT;
     if (ALLV || b < NBF) {
       const int k = b & (NS - 1);
       if (NS > 1) {
+        if (twb) {
 #pragma unroll
-        for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], __ldg(tw + (r - 1) * NS + k));
+          for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], tw[(r - 1) * NS + k]);
+        } else {
+#pragma unroll
+          for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], __ldg(tw + (r - 1) * NS + k));
+        }
       }
       Dft<R>::template apply<T, T2>(v[q]);
       const int d0 = (b - k) * R + k;
@@ -258,21 +299,22 @@ __device__ __forceinline__ void fast_stage(const fftz_pass_t &P, typename Cplx<T
 
 // Stage S of sweep SW out of NSW sweeps. GLOBALIN: the very first stage reads
 // HBM (fast kernel); the pipelined kernel has already staged the tile.
-template <typename T, int N, int S, int NST, int SW, int NSW, int FEAT, bool GLOBALIN, bool STG = false>
+template <typename T, int N, int S, int NST, int SW, int NSW, int FEAT, bool GLOBALIN, int STG = 0>
 struct FastStages {
   static __device__ __forceinline__ void run(const fftz_pass_t &P, typename Cplx<T>::type *sdata,
                                              const int64_t *s_in, const int64_t *s_out, const int64_t *s_col,
-                                             int stg_es = 1) {
+                                             int stg_es = 1, const typename Cplx<T>::type *twb = nullptr) {
     constexpr bool FIRSTG = (S == 0 && SW == 0);
     fast_stage<T, N, S, FEAT, GLOBALIN && FIRSTG, (S == NST - 1 && SW == NSW - 1), GLOBALIN && FIRSTG,
-               !GLOBALIN && FIRSTG, STG && FIRSTG>(P, sdata, s_in, s_out, s_col, stg_es);
-    FastStages<T, N, S + 1, NST, SW, NSW, FEAT, GLOBALIN, STG>::run(P, sdata, s_in, s_out, s_col, stg_es);
+               !GLOBALIN && FIRSTG, FIRSTG ? STG : 0>(P, sdata, s_in, s_out, s_col, stg_es, nullptr, nullptr, twb);
+    FastStages<T, N, S + 1, NST, SW, NSW, FEAT, GLOBALIN, STG>::run(P, sdata, s_in, s_out, s_col, stg_es, twb);
   }
 };
-template <typename T, int N, int NST, int SW, int NSW, int FEAT, bool GLOBALIN, bool STG>
+template <typename T, int N, int NST, int SW, int NSW, int FEAT, bool GLOBALIN, int STG>
 struct FastStages<T, N, NST, NST, SW, NSW, FEAT, GLOBALIN, STG> {
   static __device__ __forceinline__ void run(const fftz_pass_t &, typename Cplx<T>::type *, const int64_t *,
-                                             const int64_t *, const int64_t *, int = 1) {}
+                                             const int64_t *, const int64_t *, int = 1,
+                                             const typename Cplx<T>::type * = nullptr) {}
 };
 
 // Base offsets and column index of the transforms of one tile.
@@ -290,10 +332,17 @@ __device__ __forceinline__ void fast_tile(const fftz_pass_t &P, int64_t tf0, uns
   int64_t *s_out = s_in + P.tpc;
   int64_t *s_col = s_out + P.tpc;
   tile_offsets(P, tf0, s_in, s_out, s_col);
+  T2 *twb = nullptr;
+  if (P.smem_tw) {
+    // stage twiddles copied next to the tile: shared-memory loads in the stages
+    twb = (T2 *)(((uintptr_t)(s_col + P.tpc) + 15) & ~(uintptr_t)15);
+    const T2 *g = (const T2 *)P.tw;
+    for (int i = threadIdx.x; i < ct_tw_total(N); i += blockDim.x) twb[i] = __ldg(g + i);
+  }
   __syncthreads();
   if (FEAT & FEAT_SWEEP2) {
     constexpr int SH = Cplx<T>::PADSH;
-    FastStages<T, N, 0, ct_nstages(N), 0, 2, FEAT, true>::run(P, sdata, s_in, s_out, s_col);
+    FastStages<T, N, 0, ct_nstages(N), 0, 2, FEAT, true>::run(P, sdata, s_in, s_out, s_col, 1, twb);
     const T2 *mt = (const T2 *)P.mid_tab;
     for (int i = threadIdx.x; i < P.tpc * N; i += blockDim.x) {
       const int p = i / N;
@@ -306,9 +355,9 @@ __device__ __forceinline__ void fast_tile(const fftz_pass_t &P, int64_t tf0, uns
       *a = cmul(v, __ldg(mt + e + c * P.mid_cs));
     }
     __syncthreads();
-    FastStages<T, N, 0, ct_nstages(N), 1, 2, FEAT, true>::run(P, sdata, s_in, s_out, s_col);
+    FastStages<T, N, 0, ct_nstages(N), 1, 2, FEAT, true>::run(P, sdata, s_in, s_out, s_col, 1, twb);
   } else {
-    FastStages<T, N, 0, ct_nstages(N), 0, 1, FEAT, true>::run(P, sdata, s_in, s_out, s_col);
+    FastStages<T, N, 0, ct_nstages(N), 0, 1, FEAT, true>::run(P, sdata, s_in, s_out, s_col, 1, twb);
   }
 }
 

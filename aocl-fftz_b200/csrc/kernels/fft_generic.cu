@@ -80,10 +80,32 @@ int fftz_threads_per_transform(int dtype, int n, int nstages, const int32_t *rad
 
 int64_t fftz_smem_limit(void) { return 227 * 1024; }
 
+int32_t fftz_fast_tw_entries(int n) {
+  switch (n) {
+    case 2: return fftz::ct_tw_total(2);
+    case 4: return fftz::ct_tw_total(4);
+    case 8: return fftz::ct_tw_total(8);
+    case 16: return fftz::ct_tw_total(16);
+    case 32: return fftz::ct_tw_total(32);
+    case 64: return fftz::ct_tw_total(64);
+    case 128: return fftz::ct_tw_total(128);
+    case 256: return fftz::ct_tw_total(256);
+    case 512: return fftz::ct_tw_total(512);
+    case 1024: return fftz::ct_tw_total(1024);
+    case 2048: return fftz::ct_tw_total(2048);
+    case 4096: return fftz::ct_tw_total(4096);
+    case 8192: return fftz::ct_tw_total(8192);
+    case 16384: return fftz::ct_tw_total(16384);
+  }
+  return 0;
+}
+
 int64_t fftz_pass_smem_bytes(const fftz_pass_t *p) {
   const int64_t esz = p->dtype == 0 ? 8 : 16;
   if (is_pipe(p)) return 2 * (int64_t)p->tpc * p->sstride * esz + 9 * 8 * (int64_t)p->tpc;
-  return (int64_t)p->tpc * p->sstride * esz + 3 * 8 * (int64_t)p->tpc;
+  int64_t b = (int64_t)p->tpc * p->sstride * esz + 3 * 8 * (int64_t)p->tpc;
+  if (p->smem_tw) b += 16 + (int64_t)fftz_fast_tw_entries(p->n) * esz;  // shared copy of the stage twiddles
+  return b;
 }
 
 int fftz_launch_pass(const fftz_pass_t *p, void *stream) {

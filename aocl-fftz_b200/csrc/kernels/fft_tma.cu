@@ -111,8 +111,89 @@ __global__ void __launch_bounds__(ct_lb<T>()) fft_tma_kernel(const __grid_consta
     if (threadIdx.x == 0) atomicExch(&g_tma_wait_failed, 1);
     return;
   }
-  FastStages<T, N, 0, ct_nstages(N), 0, 1, FEAT, true, true>::run(P, sdata, s_in, s_out, s_col,
-                                                                   MODE == 1 ? tpc : 1);
+  T2 *twb = nullptr;
+  if (P.smem_tw) {
+    twb = (T2 *)(((uintptr_t)(s_col + tpc) + 15) & ~(uintptr_t)15);
+    const T2 *g = (const T2 *)P.tw;
+    for (int i = threadIdx.x; i < ct_tw_total(N); i += blockDim.x) twb[i] = __ldg(g + i);
+    __syncthreads();
+  }
+  FastStages<T, N, 0, ct_nstages(N), 0, 1, FEAT, true, 1>::run(P, sdata, s_in, s_out, s_col,
+                                                                   MODE == 1 ? tpc : 1, twb);
+}
+
+// Persistent variant: CTA b runs tiles b, b + grid, ...; while the stages of
+// tile i run, TMA copies bring the half e < N/2 of tile i + 1 into a staging
+// area beside the exchange buffer (there is not room for a whole second
+// tile); the first stage of tile i + 1 takes that half from shared memory and
+// the other half from HBM.
+template <typename T, int N, int FEAT, int MODE>
+__global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_pipe_kernel(const __grid_constant__ fftz_pass_t P,
+                                                                     const __grid_constant__ CUtensorMap tmap,
+                                                                     int64_t ntiles) {
+  typedef typename Cplx<T>::type T2;
+  constexpr int H = N / 2;
+  constexpr int HB = H < 256 ? H : 256;  // box extent along the transform
+  constexpr int CE = sizeof(T2) / 8;
+  constexpr int NST = ct_nstages(N);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  unsigned char *base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+  const int tpc = P.tpc;
+  T2 *sdata = (T2 *)base;
+  const size_t xbytes = ((size_t)tpc * P.sstride * sizeof(T2) + 127) & ~(size_t)127;
+  T2 *stg = (T2 *)(base + xbytes);
+  int64_t *s_in = (int64_t *)(stg + (size_t)tpc * H);
+  int64_t *s_out = s_in + tpc;
+  int64_t *s_col = s_out + tpc;
+  int64_t *s_stg = s_col + tpc;
+  const int64_t b0 = P.bdim[0];
+  auto issue = [&](int64_t tile) {
+    const int64_t tf0 = tile * tpc;
+    const int c0 = (int)(tf0 % b0);
+    const int z = (int)(tf0 / b0);
+    mbar_expect_tx(&bar, (unsigned)(H * tpc * sizeof(T2)));
+    if (MODE == 1) {
+      for (int k = 0; k < H / HB; k++) tma_load_3d(stg + (size_t)k * HB * tpc, &tmap, c0 * CE, k * HB, z, &bar);
+    } else {
+      for (int q = 0; q < tpc; q++)
+        for (int k = 0; k < H / HB; k++) tma_load_3d(stg + (size_t)q * H + k * HB, &tmap, k * HB * CE, c0 + q, z, &bar);
+    }
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  int64_t tile = blockIdx.x;
+  if (threadIdx.x == 0 && tile < ntiles) issue(tile);
+  for (unsigned it = 0; tile < ntiles; it++, tile += gridDim.x) {
+    for (int p = threadIdx.x; p < tpc; p += blockDim.x) {
+      batch_offsets(P, tile * tpc + p, s_in + p, s_out + p, s_col + p);
+      s_stg[p] = MODE == 1 ? p : (int64_t)p * H;
+    }
+    bool ok = false;
+    for (long i = 0; i < (1L << 22); i++)
+      if (mbar_try_wait(&bar, it & 1u)) {
+        ok = true;
+        break;
+      }
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) atomicExch(&g_tma_wait_failed, 1);
+      return;
+    }
+    fast_stage<T, N, 0, FEAT, true, NST == 1, true, false, 2>(P, sdata, s_in, s_out, s_col, MODE == 1 ? tpc : 1, stg,
+                                                              s_stg);
+    if (NST == 1) __syncthreads();
+    // every thread has read its staged half: refill the staging area
+    if (threadIdx.x == 0 && tile + gridDim.x < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(tile + gridDim.x);
+    }
+    FastStages<T, N, 1, NST, 0, 1, FEAT, true, 0>::run(P, sdata, s_in, s_out, s_col);
+    __syncthreads();
+  }
 }
 
 }  // namespace fftz
@@ -152,6 +233,25 @@ const void *pick(int n) {
   return nullptr;
 }
 
+template <typename T, int FEAT, int MODE>
+const void *pick_pipe(int n) {
+  switch (n) {
+    case 512: return (const void *)&fftz::fft_tma_pipe_kernel<T, 512, FEAT, MODE>;
+    case 1024: return (const void *)&fftz::fft_tma_pipe_kernel<T, 1024, FEAT, MODE>;
+    case 2048: return (const void *)&fftz::fft_tma_pipe_kernel<T, 2048, FEAT, MODE>;
+    case 4096: return (const void *)&fftz::fft_tma_pipe_kernel<T, 4096, FEAT, MODE>;
+  }
+  return nullptr;
+}
+
+const void *tma_pipe_kernel(int dtype, int n, int tw4, int mode) {
+  if (dtype == 0)
+    return tw4 ? (mode ? pick_pipe<float, 1, 1>(n) : pick_pipe<float, 1, 0>(n))
+               : (mode ? pick_pipe<float, 0, 1>(n) : pick_pipe<float, 0, 0>(n));
+  return tw4 ? (mode ? pick_pipe<double, 1, 1>(n) : pick_pipe<double, 1, 0>(n))
+             : (mode ? pick_pipe<double, 0, 1>(n) : pick_pipe<double, 0, 0>(n));
+}
+
 const void *tma_kernel(int dtype, int n, int tw4, int mode) {
   if (dtype == 0)
     return tw4 ? (mode ? pick<float, 1, 1>(n) : pick<float, 1, 0>(n))
@@ -174,9 +274,16 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   const int64_t b0 = p->bdim[0], b1 = p->nbdims == 2 ? p->bdim[1] : 1;
   if (p->tpc < 1 || b0 % p->tpc || p->ntf != b0 * b1) return -1;
   if (((uintptr_t)p->in & 15) != 0) return -1;
-  const void *fn = tma_kernel(p->dtype, p->n, p->variant == FFTZ_VAR_FAST_TW4, mode);
+  const int tw4 = p->variant == FFTZ_VAR_FAST_TW4;
+  int pipe = p->use_tma == 2;
+  const void *fn = pipe ? tma_pipe_kernel(p->dtype, p->n, tw4, mode) : nullptr;
+  if (!fn) {
+    pipe = 0;
+    fn = tma_kernel(p->dtype, p->n, tw4, mode);
+  }
   if (!fn || !encoder()) return -1;
-  const int64_t n = p->n, boxe = n < 256 ? n : 256;
+  const int64_t n = p->n;
+  const int64_t ext = pipe ? n / 2 : n, boxe = ext < 256 ? ext : 256;
   cuuint64_t dims[3], strides[2];
   cuuint32_t box[3], estr[3] = {1, 1, 1};
   if (mode == 1) {
@@ -211,7 +318,10 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) dev = 0;
   static int maxdyn[64][64];
-  const size_t smem = (size_t)fftz_pass_smem_bytes(p) + 128;
+  const size_t smem =
+      pipe ? ((((size_t)p->tpc * p->sstride * esz + 127) & ~(size_t)127) + (size_t)p->tpc * (n / 2) * esz +
+              4 * (size_t)p->tpc * 8 + 128)
+           : (size_t)fftz_pass_smem_bytes(p) + 128;
   int slot = -1;
   for (int i = 0; i < nopted[dev]; i++)
     if (opted[dev][i] == fn) slot = i;
@@ -230,8 +340,21 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   }
   if (slot < 0 || smem > (size_t)maxdyn[dev][slot]) return -1;
   const dim3 block((unsigned)(p->tpc * p->tpt));
-  const dim3 grid((unsigned)(p->ntf / p->tpc));
-  void *args[2] = {(void *)p, (void *)&map};
+  int64_t ntiles = p->ntf / p->tpc;
+  dim3 grid((unsigned)ntiles);
+  if (pipe) {
+    /* persistent: as many CTAs as are resident at once */
+    static int nsm[64];
+    if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, (int)block.x, smem) != cudaSuccess || occ < 1) {
+      cudaGetLastError();
+      occ = 1;
+    }
+    const int64_t cap = (int64_t)occ * (nsm[dev] > 0 ? nsm[dev] : 148);
+    grid.x = (unsigned)(ntiles < cap ? ntiles : cap);
+  }
+  void *args[3] = {(void *)p, (void *)&map, (void *)&ntiles};
   return (int)cudaLaunchKernel(fn, grid, block, args, smem, (cudaStream_t)stream);
 }
 

@@ -106,6 +106,8 @@ typedef struct fftz_pass
      * scattered through a packed ragged buffer form one batched pass */
     int32_t ind_dim;
     int32_t use_tma;                    /* fetch the tile with TMA copies when the pass qualifies */
+    int32_t smem_tw;                    /* compile-time kernels: copy the stage twiddles to shared memory */
+    int32_t pad2_;
     const int64_t *ind_in, *ind_out;
 } fftz_pass_t;
 
@@ -193,6 +195,9 @@ int fftz_pipe_max_threads(int n);
  * register budget in any stage (returns 0 if the plan is not executable). */
 int fftz_threads_per_transform(int dtype, int n, int nstages, const int32_t *radix);
 
+/* Complex entries of the stage-twiddle table of a compile-time pass of
+ * length n (0 if none). */
+int32_t fftz_fast_tw_entries(int n);
 /* Shared memory bytes used by a pass with the given tpc/sstride. */
 int64_t fftz_pass_smem_bytes(const fftz_pass_t *p);
 

@@ -55,7 +55,7 @@ class Hints(C.Structure):
     """aoclfftz_gpu_hints_t (include/aoclfftz_gpu.h)."""
     _fields_ = [("fourstep_n1", C.c_int64), ("tpc_col", C.c_int32), ("tpc_row", C.c_int32),
                 ("batch_chunk", C.c_int64), ("algorithm", C.c_int32), ("kernel_family", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("twiddles", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 def bind(lib):

@@ -60,7 +60,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=0, help="override the workload's batch (small profiling cases)")
     ap.add_argument("--fourstep-n1", type=int, default=0, help="planner hint: column length of the split")
     ap.add_argument("--tpc-col", type=int, default=0, help="planner hint: transforms per CTA, column passes")
-    ap.add_argument("--family", type=int, default=0, help="planner hint: 1 one tile per CTA, 2 persistent")
+    ap.add_argument("--family", type=int, default=0,
+                    help="planner hint: 1 plain tiles, 2 persistent, 5 TMA-fed tiles, 6 persistent TMA prefetch")
+    ap.add_argument("--twiddles", type=int, default=0, help="planner hint: 1 global, 2 shared-memory stage twiddles")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -201,6 +203,7 @@ def run_ours(args, wl):
     stream = torch.cuda.Stream()
     hints = abi.Hints()
     hints.fourstep_n1, hints.tpc_col, hints.kernel_family = args.fourstep_n1, args.tpc_col, args.family
+    hints.twiddles = args.twiddles
     lib.aoclfftz_gpu_set_hints(C.byref(hints))
     pf = make_plan(lib, abi, dx.data_ptr(), dy.data_ptr(), n, b, 0, dtype)
     pb = make_plan(lib, abi, dy.data_ptr(), dz.data_ptr(), n, b, 1, dtype)

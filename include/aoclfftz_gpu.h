@@ -58,7 +58,9 @@ FFTZ_INT32 aoclfftz_gpu_pass_info(FFTZ_VOID *handle, FFTZ_INT32 i, FFTZ_CHAR *bu
  *   kernel_family 1 one tile per CTA, loads by the threads; 2 persistent
  *                 double-buffered; 3 generic kernel only; 5 one tile per CTA
  *                 fetched by TMA copies wherever the pass qualifies
- *                 (0 = choose: TMA copies for column passes)
+ *                 (0 = choose: TMA copies for column passes); 6 persistent CTAs,
+ *                 half of the next tile prefetched by TMA
+ *   twiddles      where the stage twiddles are read from (see the field)
  * aoclfftz_gpu_set_hints(NULL) restores the defaults. */
 typedef struct aoclfftz_gpu_hints
 {
@@ -68,7 +70,9 @@ typedef struct aoclfftz_gpu_hints
     FFTZ_INT64 batch_chunk;
     FFTZ_INT32 algorithm;
     FFTZ_INT32 kernel_family;
-    FFTZ_INT32 reserved[6];
+    FFTZ_INT32 twiddles;        /* 1 stage twiddles read from global memory, 2 from a
+                                   shared-memory copy (compile-time passes >= 512 points) */
+    FFTZ_INT32 reserved[5];
 } aoclfftz_gpu_hints_t;
 
 aoclfftz_error_type aoclfftz_gpu_set_hints(const aoclfftz_gpu_hints_t *hints);

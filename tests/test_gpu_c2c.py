@@ -161,18 +161,21 @@ def test_bit_reproducible():
     for o in outs[1:]:
         assert o.tobytes() == outs[0].tobytes()
 
+@pytest.mark.parametrize("family", [5, 6])
 @pytest.mark.parametrize("dtype", ["f32", "f64"])
 @pytest.mark.parametrize("n,batch", [(1 << 16, 3), (1 << 20, 2), (1 << 24, 1), (4096, 64), (1024, 40)])
-def test_tma_fed_passes(dtype, n, batch):
-    """Kernel family 5 (tiles fetched by TMA copies) against the oracle, both
-    directions; the four-step passes qualify for column and row TMA boxes."""
+def test_tma_fed_passes(dtype, n, batch, family):
+    """Kernel families 5 (tiles fetched by TMA copies) and 6 (persistent CTAs,
+    half of the next tile prefetched by TMA during the current one) against
+    the oracle, both directions; the four-step passes qualify for column and
+    row TMA boxes."""
     if dtype == "f64" and n == 1 << 24:
         n = 1 << 22
     import aoclfftz_b200
     from aoclfftz_b200 import abi
     lib = aoclfftz_b200.load()
     h = abi.Hints()
-    h.kernel_family = 5
+    h.kernel_family = family
     lib.aoclfftz_gpu_set_hints(C.byref(h))
     try:
         for d in (0, 1):
@@ -182,3 +185,22 @@ def test_tma_fed_passes(dtype, n, batch):
                 check_c2c(dtype, [(n, 1, 1)], [(batch, n, n)], d)
     finally:
         lib.aoclfftz_gpu_set_hints(None)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n,batch", [(1 << 20, 2), (4096, 64), (512, 100)])
+def test_shared_memory_twiddles(dtype, n, batch):
+    """Hint twiddles = 2: compile-time passes of >= 512 points read their stage
+    twiddles from a shared-memory copy; results against the oracle."""
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi
+    lib = aoclfftz_b200.load()
+    h = abi.Hints()
+    h.twiddles = 2
+    lib.aoclfftz_gpu_set_hints(C.byref(h))
+    try:
+        for d in (0, 1):
+            check_c2c(dtype, [(n, 1, 1)], [(batch, n, n)], d, compare_ref=n < (1 << 20))
+    finally:
+        lib.aoclfftz_gpu_set_hints(None)
+

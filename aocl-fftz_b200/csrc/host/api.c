@@ -745,6 +745,16 @@ aoclfftz_error_type aoclfftz_gpu_synchronize(FFTZ_VOID *handle)
         return AOCLFFTZ_EXECUTION_FAILURE;
     }
     for (int i = 0; i < pl->npass; i++)
+        if (!pl->pass[i].is_elem && pl->pass[i].k.variant == FFTZ_VAR_TC)
+        {
+            if (fftz_tc_wait_failed())
+            {
+                fz_set_error("a tensor-core pass gave up waiting for its MMAs (results invalid)");
+                return AOCLFFTZ_EXECUTION_FAILURE;
+            }
+            break;
+        }
+    for (int i = 0; i < pl->npass; i++)
         if (!pl->pass[i].is_elem && pl->pass[i].k.use_tma)
         {
             if (fftz_tma_wait_failed())

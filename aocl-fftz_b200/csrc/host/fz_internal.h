@@ -131,6 +131,9 @@ int fz_bluestein_tables(fz_blob *b, int dtype, int64_t n, int64_t m, int directi
 /* appends the row-major copy T'[k1 * n2 + k2] = T[k1 + n1 * k2] of the table
  * at off; returns its offset (-1 on allocation failure) */
 int64_t fz_blob_permute(fz_blob *b, int dtype, int64_t off, int64_t n1, int64_t n2);
+/* tables of the tensor-core 4096-point kernel (DFT-64 operand halves in BF16,
+ * canonical layout, then W_4096 as float (cos, sin)); returns their offset */
+int64_t fz_tc64_tables(fz_blob *b);
 /* packed-real twiddles W_{2M}^k, k = 0..M (W^M = -1) */
 int64_t fz_real_twiddles(fz_blob *b, int dtype, int64_t M);
 

@@ -305,6 +305,20 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         fz_set_error("length %lld does not fit shared memory", (long long)n);
         return NULL;
     }
+    /* kernel_family 7: 4096-point float rows as two radix-64 tensor-core GEMM
+     * stages (split BF16 x 3; less accurate than the FP32 path, on request only) */
+    if (pl->hints.kernel_family == 7 && k->variant == FFTZ_VAR_FAST && n == 4096 && pl->dtype == 0 &&
+        k->in_mode == 0 && ies == 1 && k->ntf % 4 == 0 && (flags & ~(FFTZ_F_CONJ_IN | FFTZ_F_CONJ_OUT)) == 0)
+    {
+        k->variant = FFTZ_VAR_TC;
+        k->tpc = 4;
+        k->use_tma = 0;
+        k->smem_tw = 0;
+        p->off_tw = fz_tc64_tables(&pl->blob);
+        if (p->off_tw < 0) return NULL;
+        snprintf(p->what, sizeof(p->what), "tc n=%lld x%lld", (long long)n, (long long)k->ntf);
+        return p;
+    }
     if (k->nstages > 0)
     {
         p->off_tw = fz_stage_twiddles(&pl->blob, pl->dtype, (int)n, k->nstages, k->radix, k->tw_off);

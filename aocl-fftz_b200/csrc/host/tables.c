@@ -268,3 +268,61 @@ int64_t fz_blob_permute(fz_blob *b, int dtype, int64_t off, int64_t n1, int64_t 
             memcpy(b->p + o + (size_t)(k1 * n2 + k2) * esz, b->p + off + (size_t)(k1 + n1 * k2) * esz, esz);
     return o;
 }
+
+/* IEEE binary32 -> bfloat16 bits, round to nearest even */
+static uint16_t bf16_bits(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+static double bf16_value(uint16_t h)
+{
+    uint32_t u = (uint32_t)h << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return (double)f;
+}
+
+int64_t fz_tc64_tables(fz_blob *b)
+{
+    /* [A_hi | A_lo | W_4096]: the real 128 x 128 matrix of the 64-point DFT
+     * (rows 2k / 2k+1 = re / im of output k, columns 2j / 2j+1 = re / im of
+     * input j: [[C, S], [-S, C]], C = cos(2 pi jk/64), S = sin(2 pi jk/64)) split
+     * as hi + lo in BF16 and placed in the tensor cores' canonical K-major
+     * layout (8 x 16-byte core matrices, K-chunks 128 B apart, 8-row groups
+     * 2048 B apart); then (cos, sin)(2 pi r / 4096) for r < 4096 as floats. */
+    const size_t abytes = 128 * 256;
+    int64_t off = fz_blob_reserve(b, 2 * abytes + 4096 * 8);
+    if (off < 0) return -1;
+    unsigned char *hi = b->p + off, *lo = hi + abytes;
+    for (int row = 0; row < 128; row++)
+        for (int kk = 0; kk < 128; kk++)
+        {
+            const int k = row >> 1, j = kk >> 1;
+            double c, ms;
+            w_n((int64_t)j * k, 64, &c, &ms); /* (cos, -sin) */
+            const double sn = -ms;
+            double f;
+            if ((row & 1) == 0)
+                f = (kk & 1) == 0 ? c : sn;
+            else
+                f = (kk & 1) == 0 ? -sn : c;
+            const uint16_t h = bf16_bits((float)f);
+            const uint16_t l = bf16_bits((float)(f - bf16_value(h)));
+            const size_t o = (size_t)((row >> 3) * 2048 + (kk >> 3) * 128 + (row & 7) * 16 + (kk & 7) * 2);
+            memcpy(hi + o, &h, 2);
+            memcpy(lo + o, &l, 2);
+        }
+    float *w = (float *)(b->p + off + 2 * abytes);
+    for (int r = 0; r < 4096; r++)
+    {
+        double c, ms;
+        w_n(r, 4096, &c, &ms);
+        w[2 * r] = (float)c;
+        w[2 * r + 1] = (float)(-ms);
+    }
+    return off;
+}

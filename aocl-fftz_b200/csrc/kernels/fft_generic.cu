@@ -101,6 +101,7 @@ int32_t fftz_fast_tw_entries(int n) {
 }
 
 int64_t fftz_pass_smem_bytes(const fftz_pass_t *p) {
+  if (p->variant == FFTZ_VAR_TC) return fftz_tc_smem_bytes();
   const int64_t esz = p->dtype == 0 ? 8 : 16;
   if (is_pipe(p)) return 2 * (int64_t)p->tpc * p->sstride * esz + 9 * 8 * (int64_t)p->tpc;
   int64_t b = (int64_t)p->tpc * p->sstride * esz + 3 * 8 * (int64_t)p->tpc;
@@ -109,6 +110,7 @@ int64_t fftz_pass_smem_bytes(const fftz_pass_t *p) {
 }
 
 int fftz_launch_pass(const fftz_pass_t *p, void *stream) {
+  if (p->variant == FFTZ_VAR_TC) return fftz_launch_pass_tc(p, stream);
   if (p->use_tma) {
     const int e = fftz_launch_pass_tma(p, stream);
     if (e >= 0) return e;

@@ -51,6 +51,7 @@ enum fftz_out_kind {
 #define FFTZ_VAR_FAST_BLUE 5 /* tables plus two sweeps around a mid-table product   */
 #define FFTZ_VAR_PIPE 6      /* persistent, cp.async double-buffered, complex in/out */
 #define FFTZ_VAR_PIPE_TW4 7  /* as PIPE with the four-step twiddle epilogue         */
+#define FFTZ_VAR_TC 8        /* 4096-point rows as two radix-64 tensor-core GEMM stages */
 
 /* pass flags */
 #define FFTZ_F_CONJ_IN    0x01 /* conjugate each loaded value (after kind decode) */
@@ -217,6 +218,10 @@ int fftz_launch_pass(const fftz_pass_t *p, void *stream);
 int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream);
 /* 1 if a TMA tile gave up waiting for its copies since the last call. */
 int fftz_tma_wait_failed(void);
+/* Tensor-core form (fft_tc.cu): shared memory per CTA, launcher, wait flag. */
+int fftz_tc_smem_bytes(void);
+int fftz_launch_pass_tc(const fftz_pass_t *p, void *stream);
+int fftz_tc_wait_failed(void);
 
 #ifdef __cplusplus
 }

@@ -59,7 +59,9 @@ FFTZ_INT32 aoclfftz_gpu_pass_info(FFTZ_VOID *handle, FFTZ_INT32 i, FFTZ_CHAR *bu
  *                 double-buffered; 3 generic kernel only; 5 one tile per CTA
  *                 fetched by TMA copies wherever the pass qualifies
  *                 (0 = choose: TMA copies for column passes); 6 persistent CTAs,
- *                 half of the next tile prefetched by TMA
+ *                 half of the next tile prefetched by TMA; 7 4096-point float
+ *                 row passes as tensor-core GEMM stages (split BF16 x 3: about
+ *                 1e-5 relative error, above the FP32 path's bound)
  *   twiddles      where the stage twiddles are read from (see the field)
  * aoclfftz_gpu_set_hints(NULL) restores the defaults. */
 typedef struct aoclfftz_gpu_hints

@@ -14,6 +14,8 @@
  *   - planner flags are ignored and execute discards the status.
  */
 #include <cuda_runtime_api.h>
+#include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -383,7 +385,122 @@ static int g_nthreads = 1;
         char buf[1024];                                                                                                \
         if (aoclfftz_gpu_describe(p, buf, sizeof(buf)) >= 0 && f) fprintf(f, "%s", buf);                              \
     }                                                                                                                  \
-    void P##_print_plan(const P##_plan p) { P##_fprint_plan(p, stdout); }
+    void P##_print_plan(const P##_plan p) { P##_fprint_plan(p, stdout); }                                           \
+    /* FFTW's contract: a string the caller releases with free() */                                                 \
+    char *P##_sprint_plan(const P##_plan p)                                                                            \
+    {                                                                                                                  \
+        char buf[1024];                                                                                                \
+        buf[0] = 0;                                                                                                    \
+        if (p) aoclfftz_gpu_describe(p, buf, sizeof(buf));                                                            \
+        char *s = (char *)malloc(strlen(buf) + 1);                                                                     \
+        if (s) strcpy(s, buf);                                                                                         \
+        return s;                                                                                                      \
+    }                                                                                                                  \
+    /* nominal counts of the plan's transforms: 5 N log2 N real operations per                                       \
+     * complex transform (half for real ones), split 3 : 2 between adds and                                          \
+     * multiplies; the GPU kernels fuse many of them into FMAs */                                                    \
+    void P##_flops(const P##_plan p, double *add, double *mul, double *fmas)                                          \
+    {                                                                                                                  \
+        const double f = fw_nominal_flops(p);                                                                          \
+        if (add) *add = 0.6 * f;                                                                                       \
+        if (mul) *mul = 0.4 * f;                                                                                       \
+        if (fmas) *fmas = 0;                                                                                           \
+    }                                                                                                                  \
+    double P##_estimate_cost(const P##_plan p) { return fw_nominal_flops(p); }                                         \
+    double P##_cost(const P##_plan p) { return fw_nominal_flops(p); }                                                  \
+    int P##_alignment_of(R *p) { return (int)(((uintptr_t)p) % 16); }                                                 \
+    void P##_make_planner_thread_safe(void) {}                                                                        \
+    void P##_threads_set_callback(void (*parallel_loop)(void *(*work)(char *), char *jobdata, size_t elsize,          \
+                                                        int njobs, void *data),                                        \
+                                  void *data)                                                                          \
+    {                                                                                                                  \
+        (void)parallel_loop, (void)data; /* the GPU runs the transform, not a host thread team */                     \
+    }                                                                                                                  \
+    P##_plan P##_plan_r2r_2d(int n0, int n1, R *in, R *out, P##_r2r_kind k0, P##_r2r_kind k1, unsigned flags)         \
+    {                                                                                                                  \
+        const int n[2] = {n0, n1};                                                                                     \
+        const P##_r2r_kind k[2] = {k0, k1};                                                                            \
+        return P##_plan_r2r(2, n, in, out, k, flags);                                                                  \
+    }                                                                                                                  \
+    P##_plan P##_plan_r2r_3d(int n0, int n1, int n2, R *in, R *out, P##_r2r_kind k0, P##_r2r_kind k1,                 \
+                             P##_r2r_kind k2, unsigned flags)                                                          \
+    {                                                                                                                  \
+        const int n[3] = {n0, n1, n2};                                                                                 \
+        const P##_r2r_kind k[3] = {k0, k1, k2};                                                                        \
+        return P##_plan_r2r(3, n, in, out, k, flags);                                                                  \
+    }                                                                                                                  \
+    P##_plan P##_plan_many_r2r(int rank, const int *n, int howmany, R *in, const int *inembed, int istride,           \
+                               int idist, R *out, const int *onembed, int ostride, int odist,                          \
+                               const P##_r2r_kind *kind, unsigned flags)                                               \
+    {                                                                                                                  \
+        (void)howmany, (void)inembed, (void)istride, (void)idist, (void)onembed, (void)ostride, (void)odist;          \
+        return P##_plan_r2r(rank, n, in, out, kind, flags);                                                            \
+    }                                                                                                                  \
+    P##_plan P##_plan_guru_r2r(int rank, const P##_iodim *dims, int hr, const P##_iodim *hd, R *in, R *out,           \
+                               const P##_r2r_kind *kind, unsigned flags)                                               \
+    {                                                                                                                  \
+        (void)dims, (void)hr, (void)hd;                                                                                \
+        return P##_plan_r2r(rank, NULL, in, out, kind, flags);                                                         \
+    }                                                                                                                  \
+    P##_plan P##_plan_guru64_r2r(int rank, const P##_iodim64 *dims, int hr, const P##_iodim64 *hd, R *in, R *out,     \
+                                 const P##_r2r_kind *kind, unsigned flags)                                             \
+    {                                                                                                                  \
+        (void)dims, (void)hr, (void)hd;                                                                                \
+        return P##_plan_r2r(rank, NULL, in, out, kind, flags);                                                         \
+    }                                                                                                                  \
+    /* Wisdom: plans are rebuilt from the descriptor each time, so there is                                          \
+     * nothing to store -- exports succeed and write nothing, imports report                                         \
+     * that nothing was loaded (FFTW's "failure" value 0), and the exported                                          \
+     * string is an empty string the caller frees with free(). */                                                    \
+    void P##_forget_wisdom(void) {}                                                                                   \
+    int P##_export_wisdom_to_filename(const char *filename)                                                           \
+    {                                                                                                                  \
+        (void)filename;                                                                                                \
+        return 1;                                                                                                      \
+    }                                                                                                                  \
+    void P##_export_wisdom_to_file(FILE *f) { (void)f; }                                                              \
+    char *P##_export_wisdom_to_string(void)                                                                           \
+    {                                                                                                                  \
+        char *s = (char *)malloc(1);                                                                                   \
+        if (s) s[0] = 0;                                                                                               \
+        return s;                                                                                                      \
+    }                                                                                                                  \
+    void P##_export_wisdom(P##_write_char_func write_char, void *data) { (void)write_char, (void)data; }              \
+    int P##_import_system_wisdom(void) { return 0; }                                                                  \
+    int P##_import_wisdom_from_filename(const char *filename)                                                         \
+    {                                                                                                                  \
+        (void)filename;                                                                                                \
+        return 0;                                                                                                      \
+    }                                                                                                                  \
+    int P##_import_wisdom_from_file(FILE *f)                                                                          \
+    {                                                                                                                  \
+        (void)f;                                                                                                       \
+        return 0;                                                                                                      \
+    }                                                                                                                  \
+    int P##_import_wisdom_from_string(const char *s)                                                                  \
+    {                                                                                                                  \
+        (void)s;                                                                                                       \
+        return 0;                                                                                                      \
+    }                                                                                                                  \
+    int P##_import_wisdom(P##_read_char_func read_char, void *data)                                                   \
+    {                                                                                                                  \
+        (void)read_char, (void)data;                                                                                   \
+        return 0;                                                                                                      \
+    }                                                                                                                  \
+    const char P##_version[] = AOCLFFTZ_LIBRARY_VERSION " B200 (FFTW compatible)";
+
+/* 5 N log2 N real operations per complex transform of the plan (N the
+ * product of its dims; half for real transforms), summed over its batch */
+static double fw_nominal_flops(const void *h)
+{
+    const fz_plan *pl = (const fz_plan *)h;
+    if (!pl || pl->magic != FZ_MAGIC || pl->nop) return 0.0;
+    double n = 1.0, howmany = 1.0;
+    for (int i = 0; i < pl->sv_rank; i++) n *= (double)pl->sv_dims[i].n;
+    for (int i = 0; i < pl->sv_vrank; i++) howmany *= (double)pl->sv_vecs[i].n;
+    const double f = n > 1 ? 5.0 * n * log2(n) * howmany : 0.0;
+    return pl->fft_type == 0 ? f : 0.5 * f;
+}
 
 /* fftw_malloc: page-locked host memory (host-visible, and the library's
  * staging copies from it run at full bus speed); ordinary heap memory when

@@ -58,6 +58,10 @@ typedef struct
 typedef fftw_iodim64 fftwf_iodim64;
 typedef int fftw_r2r_kind;
 typedef int fftwf_r2r_kind;
+typedef void (*fftw_write_char_func)(char c, void *data);
+typedef int (*fftw_read_char_func)(void *data);
+typedef fftw_write_char_func fftwf_write_char_func;
+typedef fftw_read_char_func fftwf_read_char_func;
 
 /* Declares one precision's API: P = prefix tag (fftw / fftwf), R = real type,
  * C = complex type. */
@@ -114,7 +118,39 @@ typedef int fftwf_r2r_kind;
     void P##_cleanup_threads(void);                                                                        \
     void P##_set_timelimit(double t);                                                                      \
     void P##_print_plan(const P##_plan p);                                                                 \
-    void P##_fprint_plan(const P##_plan p, FILE *f);
+    void P##_fprint_plan(const P##_plan p, FILE *f);                                                       \
+    char *P##_sprint_plan(const P##_plan p);                                                               \
+    void P##_flops(const P##_plan p, double *add, double *mul, double *fmas);                              \
+    double P##_estimate_cost(const P##_plan p);                                                            \
+    double P##_cost(const P##_plan p);                                                                     \
+    int P##_alignment_of(R *p);                                                                            \
+    void P##_make_planner_thread_safe(void);                                                               \
+    void P##_threads_set_callback(void (*parallel_loop)(void *(*work)(char *), char *jobdata, size_t elsize, \
+                                                        int njobs, void *data),                            \
+                                  void *data);                                                             \
+    P##_plan P##_plan_r2r_2d(int n0, int n1, R *in, R *out, P##_r2r_kind k0, P##_r2r_kind k1, unsigned flags); \
+    P##_plan P##_plan_r2r_3d(int n0, int n1, int n2, R *in, R *out, P##_r2r_kind k0, P##_r2r_kind k1,      \
+                             P##_r2r_kind k2, unsigned flags);                                             \
+    P##_plan P##_plan_many_r2r(int rank, const int *n, int howmany, R *in, const int *inembed, int istride,  \
+                               int idist, R *out, const int *onembed, int ostride, int odist,              \
+                               const P##_r2r_kind *kind, unsigned flags);                                  \
+    P##_plan P##_plan_guru_r2r(int rank, const P##_iodim *dims, int howmany_rank,                          \
+                               const P##_iodim *howmany_dims, R *in, R *out, const P##_r2r_kind *kind,     \
+                               unsigned flags);                                                            \
+    P##_plan P##_plan_guru64_r2r(int rank, const P##_iodim64 *dims, int howmany_rank,                      \
+                                 const P##_iodim64 *howmany_dims, R *in, R *out, const P##_r2r_kind *kind, \
+                                 unsigned flags);                                                          \
+    void P##_forget_wisdom(void);                                                                          \
+    int P##_export_wisdom_to_filename(const char *filename);                                               \
+    void P##_export_wisdom_to_file(FILE *f);                                                               \
+    char *P##_export_wisdom_to_string(void);                                                               \
+    void P##_export_wisdom(P##_write_char_func write_char, void *data);                                    \
+    int P##_import_system_wisdom(void);                                                                    \
+    int P##_import_wisdom_from_filename(const char *filename);                                             \
+    int P##_import_wisdom_from_file(FILE *f);                                                              \
+    int P##_import_wisdom_from_string(const char *s);                                                      \
+    int P##_import_wisdom(P##_read_char_func read_char, void *data);                                       \
+    extern const char P##_version[];
 
 AOCLFFTZ_FFTW_DECLARE(fftw, double, fftw_complex)
 AOCLFFTZ_FFTW_DECLARE(fftwf, float, fftwf_complex)

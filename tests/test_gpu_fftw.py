@@ -153,3 +153,54 @@ def test_r2r_unsupported(libs):
     ours, _ = libs
     a = np.zeros(8)
     assert not ours.fftw_plan_r2r_1d(8, P(a), P(a), 0, EST)
+
+
+@pytest.mark.parametrize("pre", ["fftw", "fftwf"])
+def test_introspection_wisdom_and_threads(libs, pre):
+    """The ancillary FFTW calls: sprint_plan describes the GPU plan (a string
+    the caller frees), flops / cost report 5 N log2 N for the plan's batch,
+    alignment_of is the address modulo 16, wisdom export succeeds with nothing
+    written and import reports nothing loaded (as the reference wrapper), the
+    thread calls are accepted, and every r2r planner returns NULL."""
+    ours, ref = libs
+    f = lambda nm: getattr(ours, pre + "_" + nm)
+    esz = 8 if pre == "fftwf" else 16
+    a = np.zeros(2 * 4096 * 3, dtype=np.float32 if pre == "fftwf" else np.float64)
+    b = np.zeros_like(a)
+    n = (C.c_int * 1)(4096)
+    f("plan_many_dft").restype = C.c_void_p
+    p = f("plan_many_dft")(1, n, 3, P(a), None, 1, 4096, P(b), None, 1, 4096, -1, EST)
+    assert p
+    try:
+        f("sprint_plan").restype = C.c_void_p
+        sp = f("sprint_plan")(C.c_void_p(p))
+        text = C.cast(sp, C.c_char_p).value.decode()
+        assert "4096" in text, text
+        C.CDLL(None).free(C.c_void_p(sp))
+        add, mul, fma = C.c_double(), C.c_double(), C.c_double()
+        f("flops")(C.c_void_p(p), C.byref(add), C.byref(mul), C.byref(fma))
+        assert abs(add.value + mul.value - 5 * 4096 * 12 * 3) < 1e-6 and fma.value == 0
+        f("cost").restype = C.c_double
+        assert f("cost")(C.c_void_p(p)) == pytest.approx(5 * 4096 * 12 * 3)
+    finally:
+        f("destroy_plan")(C.c_void_p(p))
+    assert f("alignment_of")(C.c_void_p(a.ctypes.data + esz // 2)) == (a.ctypes.data + esz // 2) % 16
+    assert f("export_wisdom_to_filename")(b"/nonexistent/wisdom") == 1
+    f("export_wisdom_to_string").restype = C.c_void_p
+    ws = f("export_wisdom_to_string")()
+    assert C.cast(ws, C.c_char_p).value == b""
+    C.CDLL(None).free(C.c_void_p(ws))
+    assert f("import_system_wisdom")() == 0
+    assert f("import_wisdom_from_string")(b"(fftw-3.3 wisdom)") == 0
+    assert f("init_threads")() == 1
+    f("plan_with_nthreads")(4)
+    assert f("planner_nthreads")() == 4
+    f("make_planner_thread_safe")()
+    f("forget_wisdom")()
+    for nm in ("plan_r2r_2d", "plan_r2r_3d", "plan_many_r2r", "plan_guru_r2r", "plan_guru64_r2r"):
+        f(nm).restype = C.c_void_p
+    c = np.zeros(64)
+    assert not f("plan_r2r_2d")(8, 8, P(c), P(c), 0, 0, EST)
+    assert not f("plan_r2r_3d")(4, 4, 4, P(c), P(c), 0, 0, 0, EST)
+    assert (C.c_char * 16).in_dll(ours, pre + "_version").value.startswith(b"AOCL-FFTZ")
+

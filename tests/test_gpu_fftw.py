@@ -204,3 +204,48 @@ def test_introspection_wisdom_and_threads(libs, pre):
     assert not f("plan_r2r_3d")(4, 4, 4, P(c), P(c), 0, 0, 0, EST)
     assert (C.c_char * 16).in_dll(ours, pre + "_version").value.startswith(b"AOCL-FFTZ")
 
+
+def test_fortran_interface(libs):
+    """The Fortran-callable planners (arguments by reference, dimensions in
+    Fortran order): 2-D, many and guru plans of a column-major nx x ny array
+    against the oracle's 2-D DFT of the same memory viewed as [ny][nx]."""
+    ours, _ = libs
+    ref = lambda x, sg=-1: oracle.fft_nd(x.astype(np.complex128), sign=sg)
+    nx, ny, batch = 48, 20, 3
+    ip = lambda v: C.byref(C.c_int(v))
+    for fpre, dt, cd in (("dfftw", "f64", np.complex128), ("dfftwf", "f32", np.complex64)):
+        x = synthetic.complex_uniform(7, batch * nx * ny, cd)
+        y = np.zeros_like(x)
+        plan = C.c_void_p()
+        getattr(ours, fpre + "_plan_dft_2d_")(C.byref(plan), ip(nx), ip(ny), P(x), P(y), ip(-1), ip(EST))
+        assert plan.value
+        getattr(ours, fpre + "_execute_")(C.byref(plan))
+        getattr(ours, fpre + "_destroy_plan_")(C.byref(plan))
+        r = ref(x[: nx * ny].reshape(ny, nx))
+        assert oracle.rel_l2(y[: nx * ny].reshape(ny, nx), r) <= oracle.tol(nx * ny, dt)
+        # guru: n = (nx, ny), strides (1, nx), one batch dimension of distance nx * ny
+        y[:] = 0
+        n = (C.c_int * 2)(nx, ny)
+        st = (C.c_int * 2)(1, nx)
+        hn, hs = (C.c_int * 1)(batch), (C.c_int * 1)(nx * ny)
+        getattr(ours, fpre + "_plan_guru_dft_")(C.byref(plan), ip(2), n, st, st, ip(1), hn, hs, hs, P(x), P(y),
+                                                ip(-1), ip(EST))
+        assert plan.value
+        getattr(ours, fpre + "_execute_")(C.byref(plan))
+        cost = C.c_double()
+        getattr(ours, fpre + "_cost_")(C.byref(cost), C.byref(plan))
+        assert cost.value > 0
+        getattr(ours, fpre + "_destroy_plan_")(C.byref(plan))
+        for b in range(batch):
+            s_ = slice(b * nx * ny, (b + 1) * nx * ny)
+            assert oracle.rel_l2(y[s_].reshape(ny, nx), ref(x[s_].reshape(ny, nx))) <= oracle.tol(nx * ny, dt)
+        # many: rank 2, n in Fortran order, batch distance nx * ny
+        y[:] = 0
+        getattr(ours, fpre + "_plan_many_dft_")(C.byref(plan), ip(2), n, ip(batch), P(x), None, ip(1),
+                                                ip(nx * ny), P(y), None, ip(1), ip(nx * ny), ip(+1), ip(EST))
+        assert plan.value
+        getattr(ours, fpre + "_execute_")(C.byref(plan))
+        getattr(ours, fpre + "_destroy_plan_")(C.byref(plan))
+        rb = np.stack([ref(v, +1) for v in x.reshape(batch, ny, nx)])
+        assert oracle.rel_l2(y.reshape(batch, ny, nx), rb) <= oracle.tol(nx * ny, dt)
+

@@ -126,7 +126,8 @@ int fftz_launch_pass(const fftz_pass_t *p, void *stream) {
   if (nblk > 0x7fffffffLL) return (int)cudaErrorInvalidConfiguration;
   const void *fn = 0;
   if (p->variant == FFTZ_VAR_GENERIC) {
-    fn = p->dtype == 0 ? (const void *)&fftz::fft_smem_kernel<float> : (const void *)&fftz::fft_smem_kernel<double>;
+    fn = p->dtype == 0 ? (const void *)&fftz::fft_smem_kernel_occ3<float>
+                       : (const void *)&fftz::fft_smem_kernel<double>;
   } else {
     fn = fast_kernel(p->dtype, fftz::ct_log2(p->n), p->variant);
   }

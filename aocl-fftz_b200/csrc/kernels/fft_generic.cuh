@@ -27,10 +27,17 @@
 namespace fftz {
 
 // One Stockham stage of radix R over the transform this thread is mapped to.
-template <typename T, int R>
+// ROLE 0..3 fixes at compile time whether the stage reads HBM (bit 0) and
+// writes HBM (bit 1), so that the shared-memory-only middle stages compile
+// without the HBM load and epilogue code (measured on B200: float 5-15%
+// faster); ROLE 4 takes both from the runtime flags (measured faster for
+// double, whose per-role copies lose more to the call convention).
+template <typename T, int R, int ROLE>
 __device__ __noinline__ void run_stage(const fftz_pass_t &P, typename Cplx<T>::type *sdata, int s, int Ns,
-                                          bool from_g, bool to_g, int mode, const int64_t *s_in,
+                                          bool from_g_rt, bool to_g_rt, int mode, const int64_t *s_in,
                                           const int64_t *s_out, const int64_t *s_col) {
+  const bool from_g = ROLE == 4 ? from_g_rt : (ROLE & 1) != 0;
+  const bool to_g = ROLE == 4 ? to_g_rt : (ROLE & 2) != 0;
   typedef typename Cplx<T>::type T2;
   constexpr int NB = kMaxE / R;
   constexpr int SH = Cplx<T>::PADSH;
@@ -106,20 +113,39 @@ __device__ __noinline__ void run_stage(const fftz_pass_t &P, typename Cplx<T>::t
   if (!to_g) __syncthreads();
 }
 
+template <typename T, int R>
+__device__ __forceinline__ void stage_radix(const fftz_pass_t &P, typename Cplx<T>::type *sdata, int s, int Ns,
+                                            bool from_g, bool to_g, int mode, const int64_t *s_in,
+                                            const int64_t *s_out, const int64_t *s_col) {
+  if constexpr (sizeof(T) != 4) {
+    run_stage<T, R, 4>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col);
+  } else if (from_g) {
+    if (to_g)
+      run_stage<T, R, 3>(P, sdata, s, Ns, true, true, mode, s_in, s_out, s_col);
+    else
+      run_stage<T, R, 1>(P, sdata, s, Ns, true, false, mode, s_in, s_out, s_col);
+  } else {
+    if (to_g)
+      run_stage<T, R, 2>(P, sdata, s, Ns, false, true, mode, s_in, s_out, s_col);
+    else
+      run_stage<T, R, 0>(P, sdata, s, Ns, false, false, mode, s_in, s_out, s_col);
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void stage_dispatch(const fftz_pass_t &P, typename Cplx<T>::type *sdata, int s,
                                                int Ns, bool from_g, bool to_g, int mode, const int64_t *s_in,
                                                const int64_t *s_out, const int64_t *s_col) {
   switch (P.radix[s]) {
-    case 2: run_stage<T, 2>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
-    case 3: run_stage<T, 3>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
-    case 4: run_stage<T, 4>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
-    case 5: run_stage<T, 5>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
-    case 7: run_stage<T, 7>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
-    case 8: run_stage<T, 8>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
-    case 11: run_stage<T, 11>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
-    case 13: run_stage<T, 13>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
-    default: run_stage<T, 16>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    case 2: stage_radix<T, 2>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    case 3: stage_radix<T, 3>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    case 4: stage_radix<T, 4>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    case 5: stage_radix<T, 5>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    case 7: stage_radix<T, 7>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    case 8: stage_radix<T, 8>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    case 11: stage_radix<T, 11>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    case 13: stage_radix<T, 13>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
+    default: stage_radix<T, 16>(P, sdata, s, Ns, from_g, to_g, mode, s_in, s_out, s_col); break;
   }
 }
 
@@ -322,9 +348,16 @@ __device__ __forceinline__ void generic_tile(const fftz_pass_t &P, int64_t blk, 
 
 // float: at most 80 registers (3 CTAs of 256 threads per SM) -- measured on
 // B200 1.6-2.8x faster than the unbounded build for mixed-radix lines
-// (n = 1000 ... 44100); double keeps the unbounded build (no gain measured)
+// (n = 1000 ... 44100); double keeps the plain thread bound (a minimum-blocks
+// bound of 1 measured 1.7x slower for it)
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) fft_smem_kernel(const __grid_constant__ fftz_pass_t P) {
+__global__ void __launch_bounds__(256, 3) fft_smem_kernel_occ3(const __grid_constant__ fftz_pass_t P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  generic_tile<T>(P, (int64_t)blockIdx.x, smem_raw);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fft_smem_kernel(const __grid_constant__ fftz_pass_t P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   generic_tile<T>(P, (int64_t)blockIdx.x, smem_raw);
 }

@@ -68,6 +68,22 @@ def parse():
     return ap.parse_args()
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# default kernels, from one ncu capture of one 2^24-point transform
+# (profiles/fourstep24_passes_ncu.txt: pass A 231.1 MB, pass B 226.3 MB),
+# scaled to a launch over `batch` transforms (the traffic grows with them).
+TRAFFIC_PER_TRANSFORM = {("fourstep24", 0): 231.1e6, ("fourstep24", 1): 226.3e6}
+
+
+def measured_traffic(workload, args, pass_in_direction, batch):
+    """ncu-measured DRAM bytes of the dominant launch, or None when the run
+    differs from the captured configuration (hints, other workloads)."""
+    if args.family or args.fourstep_n1 or args.tpc_col or args.twiddles:
+        return None
+    t = TRAFFIC_PER_TRANSFORM.get((workload, pass_in_direction))
+    return None if t is None else round(t * batch)
+
+
 def max_over_ranks(x, ws, device="cuda"):
     """The largest value of x over all ranks (x itself on a single rank); every
     rank must call it at the same point."""
@@ -264,7 +280,9 @@ def run_ours(args, wl):
     res = dict(ms=ms, value=value, hbm_gbs=hbm_gbs, rt_err=rt_err, clocks=clk, launches=K * (npf + npb),
                buffer_bytes=total * esz,
                roofline={"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "frac": round(achieved / peak, 4),
+                         "traffic": measured_traffic(args.workload, args, dom % npf if dom < npf else (dom - npf) % npb,
+                                                     b),
                          "kernel": "%s %s" % (passes[dom][0], passes[dom][1]),
                          "bytes_per_launch": dom_bytes, "ms_per_launch": round(dom_ms, 5),
                          "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"

@@ -794,8 +794,12 @@ FFTZ_INT32 aoclfftz_gpu_describe(FFTZ_VOID *handle, FFTZ_CHAR *buf, FFTZ_INT32 l
     if (pl->rg && w < len) w += snprintf(buf + w, (size_t)(len - w), " %s", pl->rg->summary);
     for (int i = 0; i < pl->npass && w < len; i++)
         w += pl->pass[i].is_elem ? snprintf(buf + w, (size_t)(len - w), " [%s]", pl->pass[i].what)
-                                  : snprintf(buf + w, (size_t)(len - w), " [%s tpc=%d tpt=%d]", pl->pass[i].what,
-                                             pl->pass[i].k.tpc, pl->pass[i].k.tpt);
+                                  : snprintf(buf + w, (size_t)(len - w), " [%s tpc=%d tpt=%d%s]", pl->pass[i].what,
+                                             pl->pass[i].k.tpc, pl->pass[i].k.tpt,
+                                             pl->pass[i].k.use_tma == 3   ? " tma-prefetch"
+                                             : pl->pass[i].k.use_tma == 2 ? " tma-half-prefetch"
+                                             : pl->pass[i].k.use_tma      ? " tma"
+                                                                          : "");
     return w < len ? w : len - 1;
 }
 

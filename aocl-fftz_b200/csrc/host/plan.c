@@ -258,6 +258,16 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         k->use_tma = (k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4) &&
                      (fam == 5 || fam == 6 || (fam == 0 && k->in_mode == 1));
         if (k->use_tma && fam == 6) k->use_tma = 2; /* persistent, next tile half-prefetched */
+        /* persistent register-resident tiles with the next tile prefetched
+         * (4096-point float passes): by default where a column lane map
+         * makes the tile four transforms wide (measured on B200: the 2^24
+         * four-step's column pass 0.424 -> 0.324 ms, its row pass with the
+         * transposed store 0.325 -> 0.303 ms; plain rows 9% slower, so they
+         * keep the one-tile kernel), for every 4096-point float pass with
+         * kernel_family = 8 */
+        if ((k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4) && pl->dtype == 0 && n == 4096 &&
+            (fam == 8 || (fam == 0 && (k->in_mode == 1 || k->out_mode == 1))))
+            k->use_tma = 3;
         /* stage twiddles copied to shared memory by each CTA (hint twiddles = 2) */
         k->smem_tw = pl->hints.twiddles == 2 && !ragged_mode(pl) && n >= 512;
         if ((tw4 || tabs) && n < 32 && !(variant_bits & 4))

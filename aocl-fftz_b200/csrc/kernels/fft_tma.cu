@@ -196,6 +196,286 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_pipe_kernel(const __gri
   }
 }
 
+// ------------------------------------------------------- register-resident
+//
+// Persistent 4096-point float kernel whose whole next tile is in flight while
+// the current one is computed. Between stages the tile lives in registers
+// (16 complex values a thread); the stage-to-stage exchange goes through a
+// buffer holding ONE real component of the tile (x parts, then y parts), so
+// the exchange buffer (4 x 4360 floats) plus a full staged tile (4 x 4096
+// complex) fit in one SM's shared memory. Per tile: wait for the staged tile,
+// read it into registers, run stage 0 and its exchange (y parts through the
+// consumed staging area), let one thread issue the TMA copies of the next
+// tile into the staging area, then run stages 1 and 2, the last one storing
+// to HBM with the pass's epilogue.
+
+// Exchange-buffer layouts (one pad word per 2^SH words, transforms SSF words
+// apart), one per exchange of a 4096-point tile of four transforms, chosen so
+// that every access of both lane maps (rows: one transform per warp; columns:
+// four transforms per warp) touches 32 distinct banks and every per-value
+// offset is a compile-time constant: stage 0 -> 1 pads every 32 words with
+// the transforms 4228 (= 4 mod 32) words apart, stage 1 -> 2 every 16 words,
+// 4360 (= 8 mod 32). (Tiles of two transforms would let two CTAs share an SM,
+// but their 16-byte column runs made both passes 1.4-2.5x slower on B200.)
+template <int SH> __device__ __forceinline__ int rr_phys(int i) { return i + (i >> SH); }
+constexpr int kRrSh1 = 5, kRrSsf1 = 4228, kRrSh2 = 4, kRrSsf2 = 4360;
+
+template <int TPT> __device__ __forceinline__ void rr_lane(int mode, int tpc, int &p, int &j) {
+  const int t = threadIdx.x;
+  if (mode == 0) {
+    p = t / TPT;
+    j = t - p * TPT;
+  } else {
+    p = t % tpc;
+    j = t / tpc;
+  }
+}
+
+// Twiddles and butterflies of stage S on the thread's values (j under the
+// stage's lane map).
+template <typename T, int N, int S>
+__device__ __forceinline__ void rr_butterflies(const fftz_pass_t &P, typename Cplx<T>::type (&v)[16], int j) {
+  typedef typename Cplx<T>::type T2;
+  constexpr int NS = ct_ns(N, S);
+  static_assert(ct_radix(N, S) == 16, "radix-16 stages only");
+  if (NS > 1) {
+    const T2 *tw = (const T2 *)P.tw + P.tw_off[S];
+    const int k = j & (NS - 1);
+#pragma unroll
+    for (int r = 1; r < 16; r++) v[r] = cmul(v[r], __ldg(tw + (r - 1) * NS + k));
+  }
+  Dft<16>::template apply<T, T2>(v);
+}
+
+// Stage S outputs (lane map mw) -> stage S + 1 inputs (lane map mr) through
+// the one-component buffer X (layout SH, SSF). TRAIL: wait for every reader
+// before returning (another exchange of the same tile follows).
+template <typename T, int N, int S, int SH, int SSF, bool TRAIL>
+__device__ __forceinline__ void rr_exchange(T *X, typename Cplx<T>::type (&v)[16], int mw, int mr, int tpc) {
+  constexpr int NS = ct_ns(N, S);
+  constexpr int TPT = ct_tpt(N);
+  constexpr int NBF1 = N / 16;
+  // d0 + r NS and j1 + r NBF1 keep their low SH bits below 2^SH for every r,
+  // so the padded index is phys(base) + r * (stride + stride >> SH)
+  static_assert(NS == 1 ? 16 <= (1 << SH) : NS % (1 << SH) == 0, "stride vs pad");
+  static_assert(NBF1 % (1 << SH) == 0, "stride vs pad");
+  constexpr int WST = NS == 1 ? 1 : NS + (NS >> SH);
+  constexpr int RST = NBF1 + (NBF1 >> SH);
+  int p, j, p1, j1;
+  rr_lane<TPT>(mw, tpc, p, j);
+  rr_lane<TPT>(mr, tpc, p1, j1);
+  const int k = j & (NS - 1);
+  const int d0 = (j - k) * 16 + k;
+  T *xw = X + p * SSF + rr_phys<SH>(d0);
+  const T *xr = X + p1 * SSF + rr_phys<SH>(j1);
+  T tmp[16];
+#pragma unroll
+  for (int r = 0; r < 16; r++) xw[r * WST] = v[r].x;
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; r++) tmp[r] = xr[r * RST];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; r++) xw[r * WST] = v[r].y;
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    v[r].x = tmp[r];
+    v[r].y = xr[r * RST];
+  }
+  if (TRAIL) __syncthreads();
+}
+
+// Two table entries whose product is W^{(col * k) mod n} (the four-step
+// twiddle of tw4 in fft_common.cuh), fetched without multiplying them so that
+// the loads can be issued long before the product is needed.
+template <typename T>
+__device__ __forceinline__ void tw4_parts(const fftz_pass_t &P, int64_t col, int64_t k, typename Cplx<T>::type &hi,
+                                          typename Cplx<T>::type &lo) {
+  typedef typename Cplx<T>::type T2;
+  const int64_t N = P.tw4_n, L = P.tw4_l;
+  int64_t h, l;
+  if (((N & (N - 1)) == 0) && N <= 0x80000000LL && ((L & (L - 1)) == 0)) {
+    const unsigned r = ((unsigned)col * (unsigned)k) & (unsigned)(N - 1);
+    h = r >> (31 - __clz((int)L));
+    l = r & (unsigned)(L - 1);
+  } else {
+    const int64_t r = (col * k) % N;
+    h = r / L;
+    l = r - h * L;
+  }
+  hi = __ldg((const T2 *)P.tw4_hi + h);
+  lo = __ldg((const T2 *)P.tw4_lo + l);
+}
+
+// The same exchange with the y parts in a second buffer Y (same layout): one
+// barrier between the writes and the reads instead of three.
+template <typename T, int N, int S, int SH, int SSF, bool TRAIL>
+__device__ __forceinline__ void rr_exchange2(T *X, T *Y, typename Cplx<T>::type (&v)[16], int mw, int mr, int tpc) {
+  constexpr int NS = ct_ns(N, S);
+  constexpr int TPT = ct_tpt(N);
+  constexpr int NBF1 = N / 16;
+  static_assert(NS == 1 ? 16 <= (1 << SH) : NS % (1 << SH) == 0, "stride vs pad");
+  static_assert(NBF1 % (1 << SH) == 0, "stride vs pad");
+  constexpr int WST = NS == 1 ? 1 : NS + (NS >> SH);
+  constexpr int RST = NBF1 + (NBF1 >> SH);
+  int p, j, p1, j1;
+  rr_lane<TPT>(mw, tpc, p, j);
+  rr_lane<TPT>(mr, tpc, p1, j1);
+  const int k = j & (NS - 1);
+  const int d0 = (j - k) * 16 + k;
+  const int wo = p * SSF + rr_phys<SH>(d0), ro = p1 * SSF + rr_phys<SH>(j1);
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    X[wo + r * WST] = v[r].x;
+    Y[wo + r * WST] = v[r].y;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    v[r].x = X[ro + r * RST];
+    v[r].y = Y[ro + r * RST];
+  }
+  if (TRAIL) __syncthreads();
+}
+
+// Last stage's outputs to HBM (lane map out_mode) with the pass epilogue. In
+// the last radix-16 stage of 4096 points (NS = 256) thread j owns outputs
+// j + 256 r, so the four-step factor is W^{col j} (W^{256 col})^r: the
+// product hi * lo of the parts fetched at the start of the tile, then a chain
+// of products by the column's step (held in shared memory), restarted at
+// r = 8 from W^{col j} W^{2048 col}.
+template <typename T, int N, int S, int FEAT>
+__device__ __forceinline__ void rr_store(const fftz_pass_t &P, const typename Cplx<T>::type (&v)[16], int j,
+                                         int64_t obase, int64_t col, typename Cplx<T>::type hi,
+                                         typename Cplx<T>::type lo, typename Cplx<T>::type stp,
+                                         typename Cplx<T>::type stp8) {
+  typedef typename Cplx<T>::type T2;
+  constexpr int NS = ct_ns(N, S);
+  static_assert(NS * 16 == N, "last stage");
+  if (col < 0) return;
+  const int64_t oes = P.oes;
+  T2 *ob = (T2 *)P.out + obase + (int64_t)j * oes;
+  const int64_t st = (int64_t)NS * oes;
+  const bool cj = (P.flags & FFTZ_F_CONJ_OUT) != 0;
+  T2 w0 = zero2<T2>(), w = zero2<T2>();
+  if constexpr ((FEAT & FEAT_TW4) != 0) {
+    w0 = cmul(hi, lo);
+    w = w0;
+  }
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    T2 y = v[r];
+    if constexpr ((FEAT & FEAT_TW4) != 0) {
+      if (r == 8) w = cmul(w0, stp8);
+      y = cmul(y, w);
+      if (r != 7 && r != 15) w = cmul(w, stp);
+    }
+    if (cj) y.y = -y.y;
+    ob[r * st] = y;
+  }
+}
+
+template <typename T, int N, int FEAT, int MODE>
+__global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_rr_kernel(const __grid_constant__ fftz_pass_t P,
+                                                                   const __grid_constant__ CUtensorMap tmap,
+                                                                   int64_t ntiles) {
+  static_assert(N == 4096 && sizeof(T) == 4, "4096-point float tiles");
+  typedef typename Cplx<T>::type T2;
+  constexpr int TPT = ct_tpt(N);
+  constexpr int NBF = N / 16;
+  constexpr int BOXE = 256;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  unsigned char *base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+  const int tpc = P.tpc;
+  T2 *stg = (T2 *)base;                               // staged tile, TMA box layout
+  T *X = (T *)(base + (size_t)tpc * N * sizeof(T2));  // one-component exchange buffer
+  int64_t *offs = (int64_t *)(X + (size_t)tpc * kRrSsf2);  // 2 sets of {out, col} by tile parity
+  T2 *steps = (T2 *)(offs + 4 * tpc);                        // 2 sets of {W^{256 col}, W^{2048 col}}
+  const int64_t b0 = P.bdim[0];
+  auto issue = [&](int64_t tile) {
+    const int64_t tf0 = tile * tpc;
+    const int c0 = (int)(tf0 % b0);
+    const int z = (int)(tf0 / b0);
+    mbar_expect_tx(&bar, (unsigned)(N * tpc * sizeof(T2)));
+    if (MODE == 1) {
+      for (int k = 0; k < N / BOXE; k++) tma_load_3d(stg + (size_t)k * BOXE * tpc, &tmap, c0, k * BOXE, z, &bar);
+    } else {
+      for (int q = 0; q < tpc; q++)
+        for (int k = 0; k < N / BOXE; k++) tma_load_3d(stg + (size_t)q * N + k * BOXE, &tmap, k * BOXE, c0 + q, z, &bar);
+    }
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  int64_t tile = blockIdx.x;
+  if (threadIdx.x == 0 && tile < ntiles) issue(tile);
+  for (unsigned it = 0; tile < ntiles; it++, tile += gridDim.x) {
+    int64_t *s_out = offs + (size_t)(it & 1u) * 2 * tpc;
+    int64_t *s_col = s_out + tpc;
+    T2 *s_stp = steps + (size_t)(it & 1u) * 2 * tpc;
+    for (int p = threadIdx.x; p < tpc; p += blockDim.x) {
+      int64_t io;
+      batch_offsets(P, tile * tpc + p, &io, s_out + p, s_col + p);
+      if constexpr ((FEAT & FEAT_TW4) != 0) {
+        s_stp[p] = tw4<T>(P, s_col[p], N / 16);
+        s_stp[tpc + p] = tw4<T>(P, s_col[p], N / 2);
+      }
+    }
+    // bounded wait for the staged tile; a wait that gives up flags the
+    // failure for the host and ends the CTA (every thread takes one branch)
+    bool ok = false;
+    for (long i = 0; i < (1L << 22); i++)
+      if (mbar_try_wait(&bar, it & 1u)) {
+        ok = true;
+        break;
+      }
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) atomicExch(&g_tma_wait_failed, 1);
+      return;
+    }
+    T2 v[16];
+    int p, j;
+    rr_lane<TPT>(MODE, tpc, p, j);
+    {
+      const bool cj = (P.flags & FFTZ_F_CONJ_IN) != 0;
+#pragma unroll
+      for (int r = 0; r < 16; r++) {
+        const int e = j + r * NBF;
+        T2 x = MODE == 1 ? stg[(size_t)e * tpc + p] : stg[(size_t)p * N + e];
+        if (cj) x.y = -x.y;
+        v[r] = x;
+      }
+    }
+    // the four-step factor's table entries for this thread's last-stage
+    // outputs: fetched now, used after two stages
+    T2 hi = zero2<T2>(), lo = zero2<T2>();
+    if constexpr ((FEAT & FEAT_TW4) != 0) {
+      int p2, j2;
+      rr_lane<TPT>(P.out_mode, tpc, p2, j2);
+      tw4_parts<T>(P, s_col[p2], j2, hi, lo);
+    }
+    __syncthreads();  // the staged tile is consumed: its space holds exchange 1's y parts
+    rr_butterflies<T, N, 0>(P, v, j);
+    rr_exchange2<T, N, 0, kRrSh1, kRrSsf1, true>(X, (T *)stg, v, MODE, 0, tpc);
+    // the staging area is free again: bring in the next tile
+    if (threadIdx.x == 0 && tile + gridDim.x < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(tile + gridDim.x);
+    }
+    rr_lane<TPT>(0, tpc, p, j);
+    rr_butterflies<T, N, 1>(P, v, j);
+    rr_exchange<T, N, 1, kRrSh2, kRrSsf2, false>(X, v, 0, P.out_mode, tpc);
+    rr_lane<TPT>(P.out_mode, tpc, p, j);
+    rr_butterflies<T, N, 2>(P, v, j);
+    rr_store<T, N, 2, FEAT>(P, v, j, s_out[p], s_col[p], hi, lo, s_stp[p], s_stp[tpc + p]);
+  }
+}
+
 }  // namespace fftz
 
 // ------------------------------------------------------------------- host
@@ -252,6 +532,15 @@ const void *tma_pipe_kernel(int dtype, int n, int tw4, int mode) {
              : (mode ? pick_pipe<double, 0, 1>(n) : pick_pipe<double, 0, 0>(n));
 }
 
+const void *tma_rr_kernel(int dtype, int n, int tw4, int mode) {
+  if (dtype != 0 || n != 4096) return nullptr;
+  if (tw4) return mode ? (const void *)&fftz::fft_tma_rr_kernel<float, 4096, 1, 1>
+                       : (const void *)&fftz::fft_tma_rr_kernel<float, 4096, 1, 0>;
+  return mode ? (const void *)&fftz::fft_tma_rr_kernel<float, 4096, 0, 1>
+              : (const void *)&fftz::fft_tma_rr_kernel<float, 4096, 0, 0>;
+}
+
+
 const void *tma_kernel(int dtype, int n, int tw4, int mode) {
   if (dtype == 0)
     return tw4 ? (mode ? pick<float, 1, 1>(n) : pick<float, 1, 0>(n))
@@ -275,8 +564,11 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   if (p->tpc < 1 || b0 % p->tpc || p->ntf != b0 * b1) return -1;
   if (((uintptr_t)p->in & 15) != 0) return -1;
   const int tw4 = p->variant == FFTZ_VAR_FAST_TW4;
-  int pipe = p->use_tma == 2;
-  const void *fn = pipe ? tma_pipe_kernel(p->dtype, p->n, tw4, mode) : nullptr;
+  int rr = p->use_tma == 3 && p->tpc * p->tpt <= 1024;
+  const void *fn = rr ? tma_rr_kernel(p->dtype, p->n, tw4, mode) : nullptr;
+  if (!fn) rr = 0;
+  int pipe = !rr && p->use_tma == 2;
+  if (pipe) fn = tma_pipe_kernel(p->dtype, p->n, tw4, mode);
   if (!fn) {
     pipe = 0;
     fn = tma_kernel(p->dtype, p->n, tw4, mode);
@@ -319,7 +611,8 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   if (dev < 0 || dev >= 64) dev = 0;
   static int maxdyn[64][64];
   const size_t smem =
-      pipe ? ((((size_t)p->tpc * p->sstride * esz + 127) & ~(size_t)127) + (size_t)p->tpc * (n / 2) * esz +
+      rr ? ((size_t)p->tpc * n * esz + (size_t)p->tpc * fftz::kRrSsf2 * (esz / 2) + 8 * (size_t)p->tpc * 8 + 128)
+      : pipe ? ((((size_t)p->tpc * p->sstride * esz + 127) & ~(size_t)127) + (size_t)p->tpc * (n / 2) * esz +
               4 * (size_t)p->tpc * 8 + 128)
            : (size_t)fftz_pass_smem_bytes(p) + 128;
   int slot = -1;
@@ -342,7 +635,7 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   const dim3 block((unsigned)(p->tpc * p->tpt));
   int64_t ntiles = p->ntf / p->tpc;
   dim3 grid((unsigned)ntiles);
-  if (pipe) {
+  if (pipe || rr) {
     /* persistent: as many CTAs as are resident at once */
     static int nsm[64];
     if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);

@@ -187,6 +187,30 @@ def test_tma_fed_passes(dtype, n, batch, family):
         lib.aoclfftz_gpu_set_hints(None)
 
 
+@pytest.mark.parametrize("n,batch,want", [(1 << 24, 1, 2), (1 << 23, 2, 1), (4096, 64, 1), (4096, 1001, 1),
+                                          (1 << 20, 3, 0)])
+def test_register_resident_prefetch(n, batch, want):
+    """Kernel family 8: 4096-point float passes as persistent CTAs that keep
+    the tile in registers and prefetch the whole next tile by TMA. Four-step
+    2^24 runs both passes that way (column pass with the four-step twiddle,
+    row pass with the transposed store), 2^23 its 4096-point column pass,
+    plain 4096-point rows one transform per CTA; 2^20 (1024 x 1024) does not
+    qualify and keeps the default kernels. Against the oracle, both
+    directions."""
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi
+    lib = aoclfftz_b200.load()
+    h = abi.Hints()
+    h.kernel_family = 8
+    lib.aoclfftz_gpu_set_hints(C.byref(h))
+    try:
+        for d in (0, 1):
+            _, plan = check_c2c("f32", [(n, 1, 1)], [(batch, n, n)], d, compare_ref=n < (1 << 20))
+            assert plan.count("tma-prefetch") == want, plan
+    finally:
+        lib.aoclfftz_gpu_set_hints(None)
+
+
 @pytest.mark.parametrize("dtype", ["f32", "f64"])
 @pytest.mark.parametrize("n,batch", [(1 << 20, 2), (4096, 64), (512, 100)])
 def test_shared_memory_twiddles(dtype, n, batch):

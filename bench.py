@@ -70,9 +70,9 @@ def parse():
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # default kernels, from one ncu capture of one 2^24-point transform
-# (profiles/fourstep24_passes_ncu.txt: pass A 231.1 MB, pass B 226.3 MB),
+# (profiles/fourstep24_rr_passes_ncu.txt: pass A 221.2 MB, pass B 220.5 MB),
 # scaled to a launch over `batch` transforms (the traffic grows with them).
-TRAFFIC_PER_TRANSFORM = {("fourstep24", 0): 231.1e6, ("fourstep24", 1): 226.3e6}
+TRAFFIC_PER_TRANSFORM = {("fourstep24", 0): 221.2e6, ("fourstep24", 1): 220.5e6}
 
 
 def measured_traffic(workload, args, pass_in_direction, batch):

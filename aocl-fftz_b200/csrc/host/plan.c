@@ -713,21 +713,37 @@ static fz_pass *real_pass(fz_plan *pl, int64_t n0, int64_t ies, int64_t oes, con
     int64_t es_out = (k->out_kind == FFTZ_OUT_REAL_PAIRS) ? 2 * oes : oes;
     k->in_mode = (k->nbdims > 0 && absl(k->ibs[0]) < absl(es_in)) ? 1 : 0;
     k->out_mode = (k->nbdims > 0 && absl(k->obs[0]) < absl(es_out)) ? 1 : 0;
-    k->variant = FFTZ_VAR_GENERIC;
-    k->nstages = n > 1 ? generic_radices(n, k->radix) : 0;
-    if (k->nstages < 0)
+    /* power-of-two packed lines: compile-time stages between the generic
+     * load and store phases (measured on B200, fp64 512^3 r2c: the 512-point
+     * row pass at 1.14 TB/s with the generic kernel) */
+    const int fast = packed && !generic_only(pl) && is_pow2(n) && n <= fast_max_n(pl) &&
+                     !(k->flags & FFTZ_F_CONJ_IN) && fftz_fast_real_kernel(pl->dtype, ilog2i(n)) != NULL;
+    int maxthr = fftz_generic_max_threads();
+    if (fast)
     {
-        fz_set_error("real length %lld has no radix decomposition", (long long)n0);
-        return NULL;
+        k->variant = FFTZ_VAR_FAST_REAL;
+        k->nstages = fftz_fast_radices((int)n, k->radix);
+        k->tpt = fftz_fast_tpt((int)n);
+        maxthr = fast_max_threads(pl);
     }
-    k->tpt = k->nstages ? fftz_threads_per_transform(pl->dtype, (int)n, k->nstages, k->radix) : 1;
-    if (k->tpt < 1 || k->tpt > fftz_generic_max_threads())
+    else
+    {
+        k->variant = FFTZ_VAR_GENERIC;
+        k->nstages = n > 1 ? generic_radices(n, k->radix) : 0;
+        if (k->nstages < 0)
+        {
+            fz_set_error("real length %lld has no radix decomposition", (long long)n0);
+            return NULL;
+        }
+        k->tpt = k->nstages ? fftz_threads_per_transform(pl->dtype, (int)n, k->nstages, k->radix) : 1;
+    }
+    if (k->tpt < 1 || k->tpt > maxthr)
     {
         fz_set_error("real length %lld exceeds the one-pass real kernel", (long long)n0);
         return NULL;
     }
     int nslots = k->nload > n ? k->nload : (int)n;
-    finish_launch_shape(pl, k, nslots, fftz_generic_max_threads());
+    finish_launch_shape(pl, k, nslots, maxthr);
     if (fftz_pass_smem_bytes(k) > fftz_smem_limit())
     {
         fz_set_error("real length %lld does not fit shared memory", (long long)n0);

@@ -11,6 +11,7 @@ const void *fftz_fast_f64_a(int log2n, int feat);
 const void *fftz_fast_f64_b(int log2n, int feat);
 const void *fftz_fast_f32_c(int log2n, int feat);
 const void *fftz_fast_f64_c(int log2n, int feat);
+const void *fftz_fast_real_kernel(int dtype, int log2n);
 
 static const void *fast_kernel(int dtype, int log2n, int variant) {
   int feat;
@@ -22,6 +23,7 @@ static const void *fast_kernel(int dtype, int log2n, int variant) {
     case FFTZ_VAR_FAST_BLUE: feat = fftz::FEAT_TABS | fftz::FEAT_SWEEP2; break;
     case FFTZ_VAR_PIPE: feat = 16; break;
     case FFTZ_VAR_PIPE_TW4: feat = 16 | fftz::FEAT_TW4; break;
+    case FFTZ_VAR_FAST_REAL: return fftz_fast_real_kernel(dtype, log2n);
     default: return 0;
   }
   if (feat >= 16) return dtype == 0 ? fftz_fast_f32_c(log2n, feat) : fftz_fast_f64_c(log2n, feat);

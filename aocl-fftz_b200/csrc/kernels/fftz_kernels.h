@@ -52,6 +52,7 @@ enum fftz_out_kind {
 #define FFTZ_VAR_PIPE 6      /* persistent, cp.async double-buffered, complex in/out */
 #define FFTZ_VAR_PIPE_TW4 7  /* as PIPE with the four-step twiddle epilogue         */
 #define FFTZ_VAR_TC 8        /* 4096-point rows as two radix-64 tensor-core GEMM stages */
+#define FFTZ_VAR_FAST_REAL 9 /* packed real line: generic load/store phases, compile-time stages */
 
 /* pass flags */
 #define FFTZ_F_CONJ_IN    0x01 /* conjugate each loaded value (after kind decode) */
@@ -188,6 +189,9 @@ int fftz_fast_tpt(int n);
 int fftz_fast_max_n(int dtype);
 /* Radix list used by the compile-time kernel for length n (returns stages). */
 int fftz_fast_radices(int n, int32_t *radix);
+/* compile-time packed real-line kernel for complex length 2^log2n (NULL if
+ * not instantiated) */
+const void *fftz_fast_real_kernel(int dtype, int log2n);
 /* Threads per CTA the generic kernel may use; the persistent kernels' bound. */
 int fftz_generic_max_threads(void);
 int fftz_pipe_max_threads(int n);

@@ -43,6 +43,12 @@ WORKLOADS = {
                      desc="learned plan selector: seeded problems (rank 1-3, pow2 / 7-smooth / prime dims, "
                           "c2c/r2c/c2r, f32/f64, unit or strided, batch 1-256, <= 2^22 elements); candidates "
                           "timed by the autotuner; 2x64 MLP trained on 80% of problems, regret on the rest"),
+    "real3d512": dict(n=512 ** 3, batch=1, dtype="f64", real3d=(512, 512, 512),
+                      desc="r2c then c2r fp64 512^3 (FFTW order), in place, innermost rows padded to "
+                           "2 (n0/2 + 1) reals, batch 1"),
+    "real3d_256x256x1024": dict(n=256 * 256 * 1024, batch=1, dtype="f64", real3d=(256, 256, 1024),
+                                desc="r2c then c2r fp64 256 x 256 x 1024 (FFTW order), in place, innermost rows "
+                                     "padded to 2 (n0/2 + 1) reals, batch 1"),
     "ragged_f64": dict(n=0, batch=4096, dtype="f64", ragged=True,
                        desc="ragged batch of 4096 c2c fp64 transforms, lengths log-uniform in [2, 65536] "
                             "(pow2 / 7-smooth / prime thirds), packed, one persistent launch under a CUDA graph, "
@@ -334,6 +340,224 @@ def run_ours(args, wl):
     return res
 
 
+def real3d_desc(abi, ptr, shape, direction, **kw):
+    """In-place real 3-D descriptor (dims[0] innermost): r2c reads rows of
+    2 (n0/2 + 1) reals and writes n0/2 + 1 complex, c2r the reverse."""
+    n2, n1, n0 = shape
+    h0 = n0 // 2 + 1
+    rrow = 2 * h0
+    if direction == 0:
+        dims = [(n0, 1, 1), (n1, rrow, h0), (n2, rrow * n1, h0 * n1)]
+        vecs = [(1, rrow * n1 * n2, h0 * n1 * n2)]
+    else:
+        dims = [(n0, 1, 1), (n1, h0, rrow), (n2, h0 * n1, rrow * n1)]
+        vecs = [(1, h0 * n1 * n2, rrow * n1 * n2)]
+    return abi.make_desc(ptr, ptr, dims, vecs, 1, direction, 0, **kw)
+
+
+def real3d_metrics(shape, ms):
+    """2.5 N log2 N flop per direction (the reference's real-transform
+    count); algorithmic bytes per direction = N reals + (n0/2+1) n1 n2 complex."""
+    n2, n1, n0 = shape
+    N = n0 * n1 * n2
+    flop = 2 * 2.5 * N * math.log2(N)
+    byts = 2 * (N * 8 + (n0 // 2 + 1) * n1 * n2 * 16)
+    return flop / (ms * 1e-3) / 1e9, byts / (ms * 1e-3) / 1e9
+
+
+def run_real3d(args, wl):
+    """Real 3-D fp64 in place: one step = r2c then c2r (unnormalised, so the
+    round trip returns N x) through aoclfftz_execute on device buffers."""
+    import numpy as np
+    import torch
+
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi, synthetic
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    lib = aoclfftz_b200.load()
+    shape = wl["real3d"]
+    n2, n1, n0 = shape
+    N = n0 * n1 * n2
+    h0 = n0 // 2 + 1
+    x = synthetic.complex_uniform(4321 + rank, N // 2, np.complex128).view(np.float64).reshape(n2, n1, n0)
+    hx = torch.zeros((n2, n1, 2 * h0), dtype=torch.float64).pin_memory()
+    hx[:, :, :n0] = torch.from_numpy(x)
+    buf = hx.to("cuda")
+    stream = torch.cuda.Stream()
+    hints = abi.Hints()
+    hints.kernel_family = args.family
+    lib.aoclfftz_gpu_set_hints(C.byref(hints))
+    plans = []
+    for d in (0, 1):
+        desc, keep = real3d_desc(abi, buf.data_ptr(), shape, d)
+        h = abi.setup(lib, desc, "f64")
+        if not h:
+            raise RuntimeError("setup failed: %s" % lib.aoclfftz_gpu_last_error().decode())
+        lib.aoclfftz_gpu_set_stream(h, C.c_void_p(stream.cuda_stream))
+        plans.append(h)
+    pf, pb = plans
+
+    def step():
+        if lib.aoclfftz_execute(pf) or lib.aoclfftz_execute(pb):
+            raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
+
+    with torch.cuda.stream(stream):
+        step()
+    torch.cuda.synchronize()
+    xd = torch.from_numpy(x).cuda()
+    rt_err = (torch.linalg.vector_norm(buf[:, :, :n0] / N - xd) / torch.linalg.vector_norm(xd)).item()
+    del xd
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            buf[:, :, :n0] *= 1.0 / N  # keep the magnitudes from growing by N per step (outside the timing)
+            step()
+    buf.copy_(hx)
+    K = args.steps
+    lib.aoclfftz_gpu_profile_begin(pf, K)
+    lib.aoclfftz_gpu_profile_begin(pb, K)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(K):
+            step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), ws) / K
+    npf, npb = lib.aoclfftz_gpu_num_launches(pf), lib.aoclfftz_gpu_num_launches(pb)
+    tf = (C.c_float * 32)()
+    tb = (C.c_float * 32)()
+    lib.aoclfftz_gpu_profile_end(pf, tf, 32)
+    lib.aoclfftz_gpu_profile_end(pb, tb, 32)
+    value, hbm = real3d_metrics(shape, ms)
+    passes = [("fwd",) + p for p in pass_table(lib, pf)] + [("bwd",) + p for p in pass_table(lib, pb)]
+    times = [tf[i] for i in range(npf)] + [tb[i] for i in range(npb)]
+    dom = max(range(len(times)), key=lambda i: times[i])
+    dom_ms = times[dom] / K
+    dom_bytes = (passes[dom][2] + passes[dom][3]) * 16
+    peak, peak_kind = load_peaks()
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    res = dict(ms=ms, value=value * ws, hbm_gbs=hbm * ws, rt_err=rt_err, clocks=clk, launches=K * (npf + npb),
+               buffer_bytes=buf.numel() * 8,
+               roofline={"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "kernel": "%s %s" % (passes[dom][0], passes[dom][1]),
+                         "bytes_per_launch": dom_bytes, "ms_per_launch": round(dom_ms, 5),
+                         "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
+                         else "fallback 6650 GB/s"},
+               passes=[{"pass": "%s %s" % (p[0], p[1]), "ms": round(t / K, 5),
+                        "GB/s": round((p[2] + p[3]) * 16 / (t / K * 1e-3) / 1e9, 1)}
+                       for p, t in zip(passes, times)])
+    lib.aoclfftz_gpu_set_hints(None)
+    for h in plans:
+        lib.aoclfftz_destroy(h)
+    del buf
+    torch.cuda.empty_cache()
+
+    # end to end: the same two plans on the pinned host buffer (the library
+    # stages it to the device, transforms, and copies it back)
+    if not args.no_e2e:
+        eplans = []
+        for d in (0, 1):
+            desc, keep = real3d_desc(abi, hx.data_ptr(), shape, d)
+            h = abi.setup(lib, desc, "f64")
+            if not h:
+                raise RuntimeError("setup failed: %s" % lib.aoclfftz_gpu_last_error().decode())
+            lib.aoclfftz_gpu_set_stream(h, C.c_void_p(stream.cuda_stream))
+            eplans.append(h)
+
+        def estep():
+            for h in eplans:
+                if lib.aoclfftz_execute(h):
+                    raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
+
+        estep()
+        torch.cuda.synchronize()
+        e_err = float(np.linalg.norm(hx[:, :, :n0].numpy() / N - x) / np.linalg.norm(x))
+        KE = max(3, min(K, 5))
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(KE):
+            estep()
+        torch.cuda.synchronize()
+        e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / KE, ws)
+        nb = hx.numel() * 8
+        res["e2e"] = {"value": round(real3d_metrics(shape, e_ms)[0] * ws, 2), "unit": "GFLOP/s",
+                      "h2d_bytes_per_step": 2 * nb, "d2h_bytes_per_step": 2 * nb, "ms_per_step": round(e_ms, 3),
+                      "steps": KE, "round_trip_rel_l2": e_err,
+                      "api": "aoclfftz_execute with a pinned host buffer, in place (library stages H2D, FFT, D2H)"}
+        for h in eplans:
+            lib.aoclfftz_destroy(h)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return res
+
+
+def time_reference_real3d(wl, threads, steps, warmup, min_time=None):
+    """The reference's own CPU real 3-D path (r2c then c2r, in place, OpenMP)
+    on a host buffer. Returns (seconds per step, steps timed, round-trip error)."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from aoclfftz_b200 import abi, synthetic
+
+    L = oracle.ref_lib()
+    shape = wl["real3d"]
+    n2, n1, n0 = shape
+    N = n0 * n1 * n2
+    h0 = n0 // 2 + 1
+    x = synthetic.complex_uniform(99, N // 2, np.complex128).view(np.float64).reshape(n2, n1, n0)
+    buf = np.zeros((n2, n1, 2 * h0))
+    buf[:, :, :n0] = x
+    plans = []
+    for d in (0, 1):
+        desc, keep = real3d_desc(abi, buf.ctypes.data, shape, d, num_threads=threads, opt_level=3)
+        h = abi.setup(L, desc, "f64")
+        if not h:
+            raise RuntimeError("reference setup failed")
+        plans.append(h)
+
+    def step():
+        for h in plans:
+            if L.aoclfftz_execute(h) != 0:
+                raise RuntimeError("reference execute failed")
+
+    step()
+    err = float(np.linalg.norm(buf[:, :, :n0] / N - x) / np.linalg.norm(x))
+    for _ in range(warmup):
+        buf[:, :, :n0] *= 1.0 / N
+        step()
+    k = 0
+    t0 = time.perf_counter()
+    while True:
+        step()
+        k += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and k >= steps) or (min_time is not None and el >= min_time):
+            break
+    for h in plans:
+        L.aoclfftz_destroy(h)
+    return el / k, k, err
+
+
 def run_ragged(args, wl):
     """Ragged batch: one graph launch per direction (aoclfftz_gpu_ragged_*)
     against the plain path (one aoclfftz plan per transform, executed back to
@@ -547,6 +771,13 @@ def flops_per_transform(n):
 
 def cpu_baseline(wl):
     threads = os.cpu_count() or 1
+    if wl.get("real3d"):
+        sec, k, err = time_reference_real3d(wl, threads, None, 0, min_time=10.0)
+        return {"value": round(real3d_metrics(wl["real3d"], sec * 1e3)[0], 3), "unit": "GFLOP/s",
+                "cores": threads, "kind": "reference",
+                "sample": "the whole %s r2c+c2r per rep, %d reps (%.1f s), OpenMP %d threads, opt_level 3"
+                          % ("x".join(map(str, wl["real3d"])), k, sec * k, threads),
+                "round_trip_rel_l2": err}
     n = wl["n"]
     t = max(1, min(wl["batch"], (1 << 22) // n)) if n < (1 << 22) else 1
     sec, k, err = time_reference(wl, threads, t, None, 1, min_time=10.0)
@@ -568,6 +799,17 @@ def run_reference(args, wl):
     threads = os.cpu_count() or 1
     n = wl["n"]
     t = wl["batch"]
+    if wl.get("real3d"):
+        sec, k, err = time_reference_real3d(wl, threads, args.steps, args.warmup)
+        v = real3d_metrics(wl["real3d"], sec * 1e3)[0]
+        return {"metric": METRIC, "value": round(v, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"], "data": "synthetic (splitmix64 U[-1,1))",
+                "impl": "reference", "config": {"workload": wl["desc"], "n": n, "batch": 1},
+                "cpu_baseline": {"value": round(v, 3), "unit": "GFLOP/s", "cores": threads, "kind": "reference",
+                                 "sample": "the whole transform per step, r2c+c2r, OpenMP %d threads" % threads},
+                "e2e": {"value": round(v, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "round_trip_rel_l2": err}
     sec1, _, _ = time_reference(wl, threads, t, 1, 0)
     if sec1 * (args.steps + args.warmup) > 150:
         t = max(1, int(t * 150 / (sec1 * (args.steps + args.warmup))))
@@ -610,7 +852,7 @@ def main():
                               "dtype": "mixed", "data": "synthetic", "config": {"workload": wl["desc"]},
                               **r["extra"]}))
         return
-    r = run_ragged(args, wl) if wl.get("ragged") else run_ours(args, wl)
+    r = run_ragged(args, wl) if wl.get("ragged") else run_real3d(args, wl) if wl.get("real3d") else run_ours(args, wl)
     if rank != 0:
         return
     peak, peak_kind = load_peaks()

@@ -15,9 +15,13 @@
 
 namespace fftz {
 
-// Row-mapped phases with the length known at compile time (the batch index
-// of element i is a shift, pairs move as one vector access when the line is
-// aligned). Same arithmetic as the generic load_phase / store_phase.
+// Row-mapped phases with the length known at compile time: one line of the
+// tile after the other with the threads along its elements (line pointers
+// and checks hoisted), the one element a line has beyond a multiple of the
+// power-of-two length (the Nyquist bin of r2c, the middle pair of c2r) for
+// all lines in one extra step, pairs moved as one vector access when the
+// line is aligned, the half spectrum stored directly when the pass has no
+// epilogue tables. Same arithmetic as the generic load_phase / store_phase.
 
 // r2c load: real pairs (x[2e], x[2e+1]) -> Z[e]
 template <typename T, int N>
@@ -26,79 +30,100 @@ __device__ __forceinline__ void r2c_load(const fftz_pass_t &P, typename Cplx<T>:
   typedef typename Cplx<T>::type T2;
   constexpr int SH = Cplx<T>::PADSH;
   const bool cj = (P.flags & FFTZ_F_CONJ_IN) != 0;
-  for (int i = threadIdx.x; i < P.tpc * N; i += blockDim.x) {
-    const int p = i / N, e = i % N;
-    T2 x = zero2<T2>();
-    if (s_col[p] >= 0) {
-      const T *g = (const T *)P.in + s_in[p];
-      if (P.ies == 1 && ((uintptr_t)g & (sizeof(T2) - 1)) == 0) {
-        x = ((const T2 *)g)[e];
-      } else {
-        x.x = g[(int64_t)(2 * e) * P.ies];
-        x.y = g[(int64_t)(2 * e + 1) * P.ies];
+  for (int p = 0; p < P.tpc; p++) {
+    T2 *sd = sdata + (size_t)p * P.sstride;
+    const bool ok = s_col[p] >= 0;
+    const T *g = (const T *)P.in + s_in[p];
+    const bool vec = P.ies == 1 && ((uintptr_t)g & (sizeof(T2) - 1)) == 0;
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+      T2 x = zero2<T2>();
+      if (ok) {
+        if (vec) {
+          x = ((const T2 *)g)[e];
+        } else {
+          x.x = g[(int64_t)(2 * e) * P.ies];
+          x.y = g[(int64_t)(2 * e + 1) * P.ies];
+        }
+        if (cj) x.y = -x.y;
       }
-      if (cj) x.y = -x.y;
+      sd[phys<SH>(e)] = x;
     }
-    sdata[(size_t)p * P.sstride + phys<SH>(e)] = x;
   }
   __syncthreads();
 }
 
 // r2c store: X_k = (Z_k + conj Z_{N-k})/2 - (i/2) W^k (Z_k - conj Z_{N-k}), k = 0..N
 template <typename T, int N>
-__device__ __forceinline__ void r2c_store(const fftz_pass_t &P, const typename Cplx<T>::type *sdata,
-                                          const int64_t *s_out, const int64_t *s_col) {
+__device__ __forceinline__ void r2c_out(const fftz_pass_t &P, const typename Cplx<T>::type *sd, int k, int64_t col,
+                                        int64_t obase, bool plain) {
   typedef typename Cplx<T>::type T2;
   constexpr int SH = Cplx<T>::PADSH;
-  const T2 *rtw = (const T2 *)P.rtw;
-  for (int i = threadIdx.x; i < P.tpc * (N + 1); i += blockDim.x) {
-    const int p = i / (N + 1), k = i - p * (N + 1);
+  const T2 zk = sd[phys<SH>(k == N ? 0 : k)];
+  const T2 zm = sd[phys<SH>(k == 0 ? 0 : N - k)];
+  const T2 w = __ldg((const T2 *)P.rtw + k);
+  const T er = (T)0.5 * (zk.x + zm.x), ei = (T)0.5 * (zk.y - zm.y);
+  const T orr = (T)0.5 * (zk.y + zm.y), oi = (T)0.5 * (zm.x - zk.x);
+  T2 x;
+  x.x = er + (w.x * orr - w.y * oi);
+  x.y = ei + (w.x * oi + w.y * orr);
+  if (plain)
+    ((T2 *)P.out)[obase + k] = x;
+  else
+    store_complex<T>(P, x, k, col, obase);
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void r2c_store(const fftz_pass_t &P, const typename Cplx<T>::type *sdata,
+                                          const int64_t *s_out, const int64_t *s_col) {
+  const bool plain = (P.flags & (FFTZ_F_TW4 | FFTZ_F_CONJ_OUT | FFTZ_F_POST_TAB | FFTZ_F_SCALE)) == 0 &&
+                     P.post_n == 0 && P.oes == 1;
+  for (int p = 0; p < P.tpc; p++) {
     const int64_t col = s_col[p];
     if (col < 0) continue;
-    const T2 *sd = sdata + (size_t)p * P.sstride;
-    const T2 zk = sd[phys<SH>(k == N ? 0 : k)];
-    const T2 zm = sd[phys<SH>(k == 0 ? 0 : N - k)];
-    const T2 w = __ldg(rtw + k);
-    const T er = (T)0.5 * (zk.x + zm.x), ei = (T)0.5 * (zk.y - zm.y);
-    const T orr = (T)0.5 * (zk.y + zm.y), oi = (T)0.5 * (zm.x - zk.x);
-    T2 x;
-    x.x = er + (w.x * orr - w.y * oi);
-    x.y = ei + (w.x * oi + w.y * orr);
-    store_complex<T>(P, x, k, col, s_out[p]);
+    const int64_t ob = s_out[p];
+    for (int k = threadIdx.x; k < N; k += blockDim.x) r2c_out<T, N>(P, sdata + (size_t)p * P.sstride, k, col, ob, plain);
   }
+  for (int p = threadIdx.x; p < P.tpc; p += blockDim.x)  // the Nyquist bins
+    if (s_col[p] >= 0) r2c_out<T, N>(P, sdata + (size_t)p * P.sstride, N, s_col[p], s_out[p], plain);
 }
 
 // c2r load with the Hermitian separate fused: pair (k, N-k) of X[0..N] ->
 // 2 conj(Z[k]), 2 conj(Z[N-k]) (the backward conjugation included)
 template <typename T, int N>
+__device__ __forceinline__ void c2r_pair(const fftz_pass_t &P, typename Cplx<T>::type *sd,
+                                         const typename Cplx<T>::type *g, int k, bool ok) {
+  typedef typename Cplx<T>::type T2;
+  constexpr int SH = Cplx<T>::PADSH;
+  const int km = (k == 0) ? N : N - k;
+  T2 zk = zero2<T2>(), zm = zero2<T2>();
+  if (ok) {
+    const T2 xk = g[(int64_t)k * P.ies];
+    const T2 xm = g[(int64_t)km * P.ies];
+    const T2 w = __ldg((const T2 *)P.rtw + k);  // e^{-2 pi i k / 2N}
+    const T dr = xk.x - xm.x, di = xk.y + xm.y;
+    const T er = w.x * dr + w.y * di, ei = w.x * di - w.y * dr;  // conj(w) (X_k - conj X_m)
+    zk.x = (xk.x + xm.x) - ei;
+    zk.y = -((xk.y - xm.y) + er);
+    const T dr2 = xm.x - xk.x, di2 = xm.y + xk.y;
+    const T er2 = -(w.x * dr2 - w.y * di2), ei2 = -(w.x * di2 + w.y * dr2);  // -w (X_m - conj X_k)
+    zm.x = (xm.x + xk.x) - ei2;
+    zm.y = -((xm.y - xk.y) + er2);
+  }
+  if (k != 0 && km != k) sd[phys<SH>(km)] = zm;
+  sd[phys<SH>(k)] = zk;
+}
+
+template <typename T, int N>
 __device__ __forceinline__ void c2r_load(const fftz_pass_t &P, typename Cplx<T>::type *sdata, const int64_t *s_in,
                                          const int64_t *s_col) {
   typedef typename Cplx<T>::type T2;
-  constexpr int SH = Cplx<T>::PADSH;
-  constexpr int NP = N / 2 + 1;
-  const T2 *rtw = (const T2 *)P.rtw;
-  for (int i = threadIdx.x; i < P.tpc * NP; i += blockDim.x) {
-    const int p = i / NP, k = i - p * NP;
-    const int km = (k == 0) ? N : N - k;
-    T2 *sd = sdata + (size_t)p * P.sstride;
-    T2 zk = zero2<T2>(), zm = zero2<T2>();
-    if (s_col[p] >= 0) {
-      const T2 *g = (const T2 *)P.in + s_in[p];
-      const T2 xk = g[(int64_t)k * P.ies];
-      const T2 xm = g[(int64_t)km * P.ies];
-      const T2 w = __ldg(rtw + k);  // e^{-2 pi i k / 2N}
-      const T dr = xk.x - xm.x, di = xk.y + xm.y;
-      const T er = w.x * dr + w.y * di, ei = w.x * di - w.y * dr;  // conj(w) (X_k - conj X_m)
-      zk.x = (xk.x + xm.x) - ei;
-      zk.y = -((xk.y - xm.y) + er);
-      const T dr2 = xm.x - xk.x, di2 = xm.y + xk.y;
-      const T er2 = -(w.x * dr2 - w.y * di2), ei2 = -(w.x * di2 + w.y * dr2);  // -w (X_m - conj X_k)
-      zm.x = (xm.x + xk.x) - ei2;
-      zm.y = -((xm.y - xk.y) + er2);
-    }
-    if (k != 0 && km != k) sd[phys<SH>(km)] = zm;
-    sd[phys<SH>(k)] = zk;
+  for (int p = 0; p < P.tpc; p++) {
+    const bool ok = s_col[p] >= 0;
+    const T2 *g = (const T2 *)P.in + s_in[p];
+    for (int k = threadIdx.x; k < N / 2; k += blockDim.x) c2r_pair<T, N>(P, sdata + (size_t)p * P.sstride, g, k, ok);
   }
+  for (int p = threadIdx.x; p < P.tpc; p += blockDim.x)  // the middle pairs (k = N/2)
+    c2r_pair<T, N>(P, sdata + (size_t)p * P.sstride, (const T2 *)P.in + s_in[p], N / 2, s_col[p] >= 0);
   __syncthreads();
 }
 
@@ -109,21 +134,24 @@ __device__ __forceinline__ void c2r_store(const fftz_pass_t &P, const typename C
   typedef typename Cplx<T>::type T2;
   constexpr int SH = Cplx<T>::PADSH;
   const bool cj = (P.flags & FFTZ_F_CONJ_OUT) != 0, sc = (P.flags & FFTZ_F_SCALE) != 0;
-  for (int i = threadIdx.x; i < P.tpc * N; i += blockDim.x) {
-    const int p = i / N, k = i % N;
+  for (int p = 0; p < P.tpc; p++) {
     if (s_col[p] < 0) continue;
-    T2 v = sdata[(size_t)p * P.sstride + phys<SH>(k)];
-    if (cj) v.y = -v.y;
-    if (sc) {
-      v.x = (T)(v.x * P.scale);
-      v.y = (T)(v.y * P.scale);
-    }
+    const T2 *sd = sdata + (size_t)p * P.sstride;
     T *g = (T *)P.out + s_out[p];
-    if (P.oes == 1 && ((uintptr_t)g & (sizeof(T2) - 1)) == 0) {
-      ((T2 *)g)[k] = v;
-    } else {
-      g[(int64_t)(2 * k) * P.oes] = v.x;
-      g[(int64_t)(2 * k + 1) * P.oes] = v.y;
+    const bool vec = P.oes == 1 && ((uintptr_t)g & (sizeof(T2) - 1)) == 0;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+      T2 v = sd[phys<SH>(k)];
+      if (cj) v.y = -v.y;
+      if (sc) {
+        v.x = (T)(v.x * P.scale);
+        v.y = (T)(v.y * P.scale);
+      }
+      if (vec) {
+        ((T2 *)g)[k] = v;
+      } else {
+        g[(int64_t)(2 * k) * P.oes] = v.x;
+        g[(int64_t)(2 * k + 1) * P.oes] = v.y;
+      }
     }
   }
 }

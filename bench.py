@@ -67,7 +67,8 @@ def parse():
     ap.add_argument("--fourstep-n1", type=int, default=0, help="planner hint: column length of the split")
     ap.add_argument("--tpc-col", type=int, default=0, help="planner hint: transforms per CTA, column passes")
     ap.add_argument("--family", type=int, default=0,
-                    help="planner hint: 1 plain tiles, 2 persistent, 5 TMA-fed tiles, 6 persistent TMA prefetch")
+                    help="planner hint: 1 plain tiles, 2 persistent, 5 TMA-fed tiles, 6 persistent half-tile TMA "
+                         "prefetch, 7 tensor-core rows, 8 register-resident 4096-point passes everywhere")
     ap.add_argument("--twiddles", type=int, default=0, help="planner hint: 1 global, 2 shared-memory stage twiddles")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

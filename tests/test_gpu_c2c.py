@@ -128,8 +128,11 @@ def test_host_buffers_and_ilp64():
 def test_pinned_host_buffers_pipelined():
     """Page-locked host buffers take the chunked copy-in / passes / copy-out
     pipeline (three streams); results must match the oracle exactly as the
-    device path does."""
+    device path does. Four-step lines (2^18 f64, 2^22 and 2^24 f32) run their
+    last pass in blocks of columns, each copied out behind it."""
     check_c2c("f32", [(4096, 1, 1)], [(64, 4096, 4096)], 0, host=True, pinned=True, compare_ref=False)
+    check_c2c("f32", [(1 << 22, 1, 1)], [(3, 1 << 22, 1 << 22)], 0, host=True, pinned=True, compare_ref=False)
+    check_c2c("f32", [(1 << 24, 1, 1)], [(2, 1 << 24, 1 << 24)], 1, host=True, pinned=True, compare_ref=False)
     check_c2c("f64", [(1 << 18, 1, 1)], [(4, 1 << 18, 1 << 18)], 1, host=True, pinned=True, compare_ref=False)
     check_c2c("f32", [(100, 1, 1)], [(48, 130, 100)], 0, host=True, pinned=True)
     check_c2c("f64", [(256, 1, 1)], [(12, 256, 256)], 1, placement=0, host=True, pinned=True)

@@ -109,3 +109,33 @@ def test_r2c_c2r_multipass_lines(dtype, n):
 def test_r2c_c2r_multipass_inplace_nd():
     check_real("f32", [4, 34], batch=2, inplace=True)
     check_real("f64", [3, 17], batch=1)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n", [16, 256, 1024])
+def test_r2c_c2r_interleaved_batch(dtype, n):
+    """Transforms interleaved element by element (element stride = batch,
+    distance 1): the real lines take a column lane map, so the compile-time
+    real-line kernel runs the generic load and store phases around its
+    stages. Both directions against the oracle."""
+    B = 8
+    h0 = n // 2 + 1
+    tol = oracle.tol(n, dtype)
+    x = synthetic.normal(11, B * n).reshape(B, n).astype(real_dtype(dtype))
+    dims, vecs = [(n, B, B)], [(B, 1, 1)]
+    in_sc = span(dims, vecs, "in")
+    out_sc = 2 * span(dims, vecs, "out", n0=h0)
+    raw = scatter(x, [(n, B)], [(B, 1)], in_sc, dtype, complex_side=False)
+    out_raw, plan = run_gpu(dtype, dims, vecs, raw, out_sc, 1, 0, 1)
+    X = gather(out_raw, [(n, B)], [(B, 1)], dtype, n0=h0)
+    ref = oracle.rfftn(x.astype(np.float64), rank=1)
+    err = oracle.rel_l2(X, ref)
+    assert err <= tol, "r2c rel-L2 %.3e > %.3e; plan %s" % (err, tol, plan)
+    cin_sc = 2 * span(dims, vecs, "in", n0=h0)
+    cout_sc = span(dims, vecs, "out")
+    craw = scatter(ref.astype(np.complex64 if dtype == "f32" else np.complex128), [(n, B)], [(B, 1)], cin_sc, dtype,
+                   n0=h0)
+    y_raw, plan2 = run_gpu(dtype, dims, vecs, craw, cout_sc, 1, 1, 1)
+    y = gather(y_raw, [(n, B)], [(B, 1)], dtype, complex_side=False)
+    err2 = oracle.rel_l2(y, x.astype(np.float64) * n)
+    assert err2 <= tol, "c2r rel-L2 %.3e > %.3e; plan %s" % (err2, tol, plan2)

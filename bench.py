@@ -391,7 +391,7 @@ def run_real3d(args, wl):
     buf = hx.to("cuda")
     stream = torch.cuda.Stream()
     hints = abi.Hints()
-    hints.kernel_family = args.family
+    hints.kernel_family, hints.tpc_col, hints.twiddles = args.family, args.tpc_col, args.twiddles
     lib.aoclfftz_gpu_set_hints(C.byref(hints))
     plans = []
     for d in (0, 1):

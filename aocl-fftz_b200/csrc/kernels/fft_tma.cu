@@ -209,16 +209,15 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_pipe_kernel(const __gri
 // tile into the staging area, then run stages 1 and 2, the last one storing
 // to HBM with the pass's epilogue.
 
-// Exchange-buffer layouts (one pad word per 2^SH words, transforms SSF words
-// apart), one per exchange of a 4096-point tile of four transforms, chosen so
-// that every access of both lane maps (rows: one transform per warp; columns:
-// four transforms per warp) touches 32 distinct banks and every per-value
-// offset is a compile-time constant: stage 0 -> 1 pads every 32 words with
-// the transforms 4228 (= 4 mod 32) words apart, stage 1 -> 2 every 16 words,
-// 4360 (= 8 mod 32). (Tiles of two transforms would let two CTAs share an SM,
-// but their 16-byte column runs made both passes 1.4-2.5x slower on B200.)
+// Exchange 1's buffer layout (one pad word per 2^SH words, transforms SSF
+// words apart): SH = 5 with the transforms 4228 (= 4 mod 32) words apart puts
+// every access of both lane maps (rows: one transform per warp; columns: four
+// transforms per warp) on 32 distinct banks with compile-time per-value
+// offsets (checked by a simulation of every access). (Tiles of two transforms
+// would let two CTAs share an SM, but their 16-byte column runs made both
+// passes 1.4-2.5x slower on B200.)
 template <int SH> __device__ __forceinline__ int rr_phys(int i) { return i + (i >> SH); }
-constexpr int kRrSh1 = 5, kRrSsf1 = 4228, kRrSh2 = 4, kRrSsf2 = 4360;
+constexpr int kRrSh1 = 5, kRrSsf1 = 4228;
 
 template <int TPT> __device__ __forceinline__ void rr_lane(int mode, int tpc, int &p, int &j) {
   const int t = threadIdx.x;
@@ -247,69 +246,10 @@ __device__ __forceinline__ void rr_butterflies(const fftz_pass_t &P, typename Cp
   Dft<16>::template apply<T, T2>(v);
 }
 
-// Stage S outputs (lane map mw) -> stage S + 1 inputs (lane map mr) through
-// the one-component buffer X (layout SH, SSF). TRAIL: wait for every reader
-// before returning (another exchange of the same tile follows).
-template <typename T, int N, int S, int SH, int SSF, bool TRAIL>
-__device__ __forceinline__ void rr_exchange(T *X, typename Cplx<T>::type (&v)[16], int mw, int mr, int tpc) {
-  constexpr int NS = ct_ns(N, S);
-  constexpr int TPT = ct_tpt(N);
-  constexpr int NBF1 = N / 16;
-  // d0 + r NS and j1 + r NBF1 keep their low SH bits below 2^SH for every r,
-  // so the padded index is phys(base) + r * (stride + stride >> SH)
-  static_assert(NS == 1 ? 16 <= (1 << SH) : NS % (1 << SH) == 0, "stride vs pad");
-  static_assert(NBF1 % (1 << SH) == 0, "stride vs pad");
-  constexpr int WST = NS == 1 ? 1 : NS + (NS >> SH);
-  constexpr int RST = NBF1 + (NBF1 >> SH);
-  int p, j, p1, j1;
-  rr_lane<TPT>(mw, tpc, p, j);
-  rr_lane<TPT>(mr, tpc, p1, j1);
-  const int k = j & (NS - 1);
-  const int d0 = (j - k) * 16 + k;
-  T *xw = X + p * SSF + rr_phys<SH>(d0);
-  const T *xr = X + p1 * SSF + rr_phys<SH>(j1);
-  T tmp[16];
-#pragma unroll
-  for (int r = 0; r < 16; r++) xw[r * WST] = v[r].x;
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < 16; r++) tmp[r] = xr[r * RST];
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < 16; r++) xw[r * WST] = v[r].y;
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < 16; r++) {
-    v[r].x = tmp[r];
-    v[r].y = xr[r * RST];
-  }
-  if (TRAIL) __syncthreads();
-}
-
-// Two table entries whose product is W^{(col * k) mod n} (the four-step
-// twiddle of tw4 in fft_common.cuh), fetched without multiplying them so that
-// the loads can be issued long before the product is needed.
-template <typename T>
-__device__ __forceinline__ void tw4_parts(const fftz_pass_t &P, int64_t col, int64_t k, typename Cplx<T>::type &hi,
-                                          typename Cplx<T>::type &lo) {
-  typedef typename Cplx<T>::type T2;
-  const int64_t N = P.tw4_n, L = P.tw4_l;
-  int64_t h, l;
-  if (((N & (N - 1)) == 0) && N <= 0x80000000LL && ((L & (L - 1)) == 0)) {
-    const unsigned r = ((unsigned)col * (unsigned)k) & (unsigned)(N - 1);
-    h = r >> (31 - __clz((int)L));
-    l = r & (unsigned)(L - 1);
-  } else {
-    const int64_t r = (col * k) % N;
-    h = r / L;
-    l = r - h * L;
-  }
-  hi = __ldg((const T2 *)P.tw4_hi + h);
-  lo = __ldg((const T2 *)P.tw4_lo + l);
-}
-
-// The same exchange with the y parts in a second buffer Y (same layout): one
-// barrier between the writes and the reads instead of three.
+// Stage S outputs (lane map mw) -> stage S + 1 inputs (lane map mr) with the
+// x parts in X and the y parts in Y (both in layout SH, SSF): one barrier
+// between the writes and the reads. TRAIL: wait for every reader before
+// returning (the buffers are written again after it).
 template <typename T, int N, int S, int SH, int SSF, bool TRAIL>
 __device__ __forceinline__ void rr_exchange2(T *X, T *Y, typename Cplx<T>::type (&v)[16], int mw, int mr, int tpc) {
   constexpr int NS = ct_ns(N, S);
@@ -337,6 +277,66 @@ __device__ __forceinline__ void rr_exchange2(T *X, T *Y, typename Cplx<T>::type 
     v[r].y = Y[ro + r * RST];
   }
   if (TRAIL) __syncthreads();
+}
+
+// Exchange 2 (stage 1, row map, outputs d0 + 16 r -> stage 2 inputs j1 + 256 r)
+// through X in an unpadded layout: element i of transform p at p * 4096 +
+// (i ^ (bit 8 of i) << 4 ^ 8 p), bank-conflict-free for row and column read
+// maps (64 KB for four transforms instead of the padded layout's 68 KB, which
+// keeps the CTA under the 196 KB shared-memory carveout and leaves L1 60 KB
+// for the twiddle tables). Each thread needs two base offsets (even and odd
+// r) with compile-time steps.
+template <typename T, int N>
+__device__ __forceinline__ void rr_exchange_x(T *X, typename Cplx<T>::type (&v)[16], int mr, int tpc) {
+  static_assert(N == 4096 && ct_ns(N, 1) == 16, "4096 = 16 x 16 x 16");
+  constexpr int TPT = ct_tpt(N);
+  int p, j, p1, j1;
+  rr_lane<TPT>(0, tpc, p, j);
+  rr_lane<TPT>(mr, tpc, p1, j1);
+  // writes: i = 256 a + c + 16 r (a = j / 16, c = j % 16); bit 8 of i is a & 1
+  const int key = (((j >> 4) & 1) << 4) ^ (8 * p);
+  const int kb = key >> 4 & 1;
+  const int wb = p * 4096 + ((((j >> 4) << 8) + (j & 15)) ^ (key & 8));
+  const int we = wb + 16 * kb, wo = wb - 16 * kb;
+  // reads: i = j1 + 256 r; bit 8 of i is r & 1
+  const int re = p1 * 4096 + (j1 ^ (8 * p1)), ro = re ^ 16;
+  T tmp[16];
+#pragma unroll
+  for (int r = 0; r < 16; r++) X[((r & 1) ? wo : we) + 16 * r] = v[r].x;
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; r++) tmp[r] = X[((r & 1) ? ro : re) + 256 * r];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; r++) X[((r & 1) ? wo : we) + 16 * r] = v[r].y;
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    v[r].x = tmp[r];
+    v[r].y = X[((r & 1) ? ro : re) + 256 * r];
+  }
+}
+
+// Two table entries whose product is W^{(col * k) mod n} (the four-step
+// twiddle of tw4 in fft_common.cuh), fetched without multiplying them so that
+// the loads can be issued long before the product is needed.
+template <typename T>
+__device__ __forceinline__ void tw4_parts(const fftz_pass_t &P, int64_t col, int64_t k, typename Cplx<T>::type &hi,
+                                          typename Cplx<T>::type &lo) {
+  typedef typename Cplx<T>::type T2;
+  const int64_t N = P.tw4_n, L = P.tw4_l;
+  int64_t h, l;
+  if (((N & (N - 1)) == 0) && N <= 0x80000000LL && ((L & (L - 1)) == 0)) {
+    const unsigned r = ((unsigned)col * (unsigned)k) & (unsigned)(N - 1);
+    h = r >> (31 - __clz((int)L));
+    l = r & (unsigned)(L - 1);
+  } else {
+    const int64_t r = (col * k) % N;
+    h = r / L;
+    l = r - h * L;
+  }
+  hi = __ldg((const T2 *)P.tw4_hi + h);
+  lo = __ldg((const T2 *)P.tw4_lo + l);
 }
 
 // Last stage's outputs to HBM (lane map out_mode) with the pass epilogue. In
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_rr_kernel(const __grid_
   const int tpc = P.tpc;
   T2 *stg = (T2 *)base;                               // staged tile, TMA box layout
   T *X = (T *)(base + (size_t)tpc * N * sizeof(T2));  // one-component exchange buffer
-  int64_t *offs = (int64_t *)(X + (size_t)tpc * kRrSsf2);  // 2 sets of {out, col} by tile parity
+  int64_t *offs = (int64_t *)(X + (size_t)tpc * kRrSsf1);  // 2 sets of {out, col} by tile parity
   T2 *steps = (T2 *)(offs + 4 * tpc);                        // 2 sets of {W^{256 col}, W^{2048 col}}
   const int64_t b0 = P.bdim[0];
   auto issue = [&](int64_t tile) {
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_rr_kernel(const __grid_
     }
     rr_lane<TPT>(0, tpc, p, j);
     rr_butterflies<T, N, 1>(P, v, j);
-    rr_exchange<T, N, 1, kRrSh2, kRrSsf2, false>(X, v, 0, P.out_mode, tpc);
+    rr_exchange_x<T, N>(X, v, P.out_mode, tpc);
     rr_lane<TPT>(P.out_mode, tpc, p, j);
     rr_butterflies<T, N, 2>(P, v, j);
     rr_store<T, N, 2, FEAT>(P, v, j, s_out[p], s_col[p], hi, lo, s_stp[p], s_stp[tpc + p]);
@@ -611,7 +611,7 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   if (dev < 0 || dev >= 64) dev = 0;
   static int maxdyn[64][64];
   const size_t smem =
-      rr ? ((size_t)p->tpc * n * esz + (size_t)p->tpc * fftz::kRrSsf2 * (esz / 2) + 8 * (size_t)p->tpc * 8 + 128)
+      rr ? ((size_t)p->tpc * n * esz + (size_t)p->tpc * fftz::kRrSsf1 * (esz / 2) + 8 * (size_t)p->tpc * 8 + 128)
       : pipe ? ((((size_t)p->tpc * p->sstride * esz + 127) & ~(size_t)127) + (size_t)p->tpc * (n / 2) * esz +
               4 * (size_t)p->tpc * 8 + 128)
            : (size_t)fftz_pass_smem_bytes(p) + 128;

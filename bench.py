@@ -43,6 +43,8 @@ WORKLOADS = {
                      desc="learned plan selector: seeded problems (rank 1-3, pow2 / 7-smooth / prime dims, "
                           "c2c/r2c/c2r, f32/f64, unit or strided, batch 1-256, <= 2^22 elements); candidates "
                           "timed by the autotuner; 2x64 MLP trained on 80% of problems, regret on the rest"),
+    "mixed1000": dict(n=1000, batch=32768, dtype="f32",
+                      desc="c2c fp32 N=1000 (2^3 5^3, mixed radix) batch 32768, out-of-place, fwd+bwd"),
     "real3d512": dict(n=512 ** 3, batch=1, dtype="f64", real3d=(512, 512, 512),
                       desc="r2c then c2r fp64 512^3 (FFTW order), in place, innermost rows padded to "
                            "2 (n0/2 + 1) reals, batch 1"),

@@ -200,14 +200,15 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_pipe_kernel(const __gri
 //
 // Persistent 4096-point float kernel whose whole next tile is in flight while
 // the current one is computed. Between stages the tile lives in registers
-// (16 complex values a thread); the stage-to-stage exchange goes through a
+// (16 complex values a thread); a stage-to-stage exchange goes through a
 // buffer holding ONE real component of the tile (x parts, then y parts), so
-// the exchange buffer (4 x 4360 floats) plus a full staged tile (4 x 4096
-// complex) fit in one SM's shared memory. Per tile: wait for the staged tile,
-// read it into registers, run stage 0 and its exchange (y parts through the
-// consumed staging area), let one thread issue the TMA copies of the next
-// tile into the staging area, then run stages 1 and 2, the last one storing
-// to HBM with the pass's epilogue.
+// the exchange buffer (4 x 4228 floats) plus a full staged tile (4 x 4096
+// complex) fit in one SM's shared memory (199 KB). Per tile: wait for the
+// staged tile, read it into registers, run stage 0 and exchange 1 (its y
+// parts through the consumed staging area, so one barrier between writes and
+// reads), let one thread issue the TMA copies of the next tile into the
+// staging area, then run stage 1, exchange 2 (x then y through the exchange
+// buffer) and stage 2, which stores to HBM with the pass's epilogue.
 
 // Exchange 1's buffer layout (one pad word per 2^SH words, transforms SSF
 // words apart): SH = 5 with the transforms 4228 (= 4 mod 32) words apart puts

@@ -68,6 +68,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=0, help="override the workload's batch (small profiling cases)")
     ap.add_argument("--fourstep-n1", type=int, default=0, help="planner hint: column length of the split")
     ap.add_argument("--tpc-col", type=int, default=0, help="planner hint: transforms per CTA, column passes")
+    ap.add_argument("--tpc-row", type=int, default=0, help="planner hint: transforms per CTA, row passes")
     ap.add_argument("--family", type=int, default=0,
                     help="planner hint: 1 plain tiles, 2 persistent, 5 TMA-fed tiles, 6 persistent half-tile TMA "
                          "prefetch, 7 tensor-core rows, 8 register-resident 4096-point passes everywhere")
@@ -87,7 +88,7 @@ TRAFFIC_PER_TRANSFORM = {("fourstep24", 0): 221.2e6, ("fourstep24", 1): 220.5e6}
 def measured_traffic(workload, args, pass_in_direction, batch):
     """ncu-measured DRAM bytes of the dominant launch, or None when the run
     differs from the captured configuration (hints, other workloads)."""
-    if args.family or args.fourstep_n1 or args.tpc_col or args.twiddles:
+    if args.family or args.fourstep_n1 or args.tpc_col or args.tpc_row or args.twiddles:
         return None
     t = TRAFFIC_PER_TRANSFORM.get((workload, pass_in_direction))
     return None if t is None else round(t * batch)
@@ -228,6 +229,7 @@ def run_ours(args, wl):
     stream = torch.cuda.Stream()
     hints = abi.Hints()
     hints.fourstep_n1, hints.tpc_col, hints.kernel_family = args.fourstep_n1, args.tpc_col, args.family
+    hints.tpc_row = args.tpc_row
     hints.twiddles = args.twiddles
     lib.aoclfftz_gpu_set_hints(C.byref(hints))
     pf = make_plan(lib, abi, dx.data_ptr(), dy.data_ptr(), n, b, 0, dtype)
@@ -393,7 +395,8 @@ def run_real3d(args, wl):
     buf = hx.to("cuda")
     stream = torch.cuda.Stream()
     hints = abi.Hints()
-    hints.kernel_family, hints.tpc_col, hints.twiddles = args.family, args.tpc_col, args.twiddles
+    hints.kernel_family, hints.tpc_col, hints.tpc_row = args.family, args.tpc_col, args.tpc_row
+    hints.twiddles = args.twiddles
     lib.aoclfftz_gpu_set_hints(C.byref(hints))
     plans = []
     for d in (0, 1):

@@ -4,7 +4,12 @@
 Default workload (one step = forward then backward, unnormalised):
   c2c fp32, N = 2^24 = 4096 x 4096 (four-step: two passes through HBM),
   batch 4, out of place; inputs re, im i.i.d. U[-1, 1) from a seed.
-Other workloads (--workload): "batch4096" (N = 4096, batch 1024, one pass).
+Other workloads (--workload): "batch4096" (N = 4096, batch 1024, one pass);
+"mixed1000" (N = 1000 = 2^3 5^3, batch 32768, the mixed-radix kernel);
+"ragged" / "ragged_f64" (4096 transforms of lengths in [2, 65536] in one
+persistent launch); "real3d512" / "real3d_256x256x1024" (fp64 real 3-D, in
+place, r2c then c2r, 2.5 N log2 N per direction); "selector" (regret of the
+learned plan selector).
 
 Metric: 5 N log2(N) GFLOP/s over all transforms of the step (both directions),
 plus HBM GB/s. `value` is measured with inputs resident in HBM; `e2e` runs the

@@ -278,6 +278,16 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         if ((k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4) && pl->dtype == 0 && n == 4096 &&
             (fam == 8 || (fam == 0 && (k->in_mode == 1 || k->out_mode == 1))))
             k->use_tma = 3;
+        /* 16 x 256 split tiles (persistent, one exchange across the CTA per
+         * tile): by default where the register-resident kernel was (measured
+         * on B200, 2^24 four-step: column pass 0.300 -> 0.290 ms, row pass
+         * with the transposed store 0.301 -> 0.251 ms), for every 4096-point
+         * float pass with kernel_family 9 (one real component per exchange
+         * round) or 10 (full complex values in two rounds, round-1 readers'
+         * values stashed in shared memory: 0.326 / 0.282 ms) */
+        if ((k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4) && pl->dtype == 0 && n == 4096 &&
+            (fam == 9 || fam == 10 || (fam == 0 && (k->in_mode == 1 || k->out_mode == 1))))
+            k->use_tma = fam == 10 ? 5 : 4;
         /* stage twiddles copied to shared memory by each CTA (hint twiddles = 2) */
         k->smem_tw = pl->hints.twiddles == 2 && !ragged_mode(pl) && n >= 512;
         if ((tw4 || tabs) && n < 32 && !(variant_bits & 4))
@@ -312,6 +322,11 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
     int nslots = (int)n;
     if (k->nload > nslots) nslots = k->nload;
     finish_launch_shape(pl, k, nslots, maxthr);
+    /* split tiles hold four transforms: row passes take four per CTA too when
+     * whole tiles cover the first batch dimension */
+    if (k->use_tma >= 4 && k->tpc < 4 && pl->hints.tpc_row == 0 && k->nbdims > 0 && k->bdim[0] % 4 == 0)
+        k->tpc = 4;
+    if (k->use_tma >= 4 && k->tpc != 4) k->use_tma = 3; /* no whole tiles: register-resident kernel */
     if (is_pipe_variant(k->variant) && fftz_pass_smem_bytes(k) > fftz_smem_limit())
     {
         /* two slots do not fit: the one-tile-per-CTA kernel of the same shape */

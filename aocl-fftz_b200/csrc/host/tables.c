@@ -125,6 +125,10 @@ int fz_tw4_tables(fz_blob *b, int dtype, int64_t N, int64_t *L, int64_t *off_hi,
      * the working precision (the product is taken in the working precision) */
     int64_t l = 1;
     while (l * l < N) l *= 2;
+    /* lo holds at most 1024 factors while hi stays <= 2^20 entries: the
+     * four-step epilogue's random lookups (r = column * k) then stay within
+     * two 1024-entry tables that remain in L1 beside the stage twiddles */
+    if (l > 1024 && (N + 1023) / 1024 <= ((int64_t)1 << 20)) l = 1024;
     int64_t nhi = (N + l - 1) / l;
     size_t esz = dtype == 0 ? 8 : 16;
     *L = l;

@@ -57,6 +57,26 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
+// Stores of the persistent kernels' outputs do not allocate in L1 (128 KB of
+// output per tile would evict the twiddle tables), and twiddle loads are kept
+// in L1 with the evict-last priority.
+__device__ __forceinline__ void st_na(float2 *p, float2 v) {
+  asm volatile("st.global.L1::no_allocate.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void st_na(double2 *p, double2 v) {
+  asm volatile("st.global.L1::no_allocate.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.x), "d"(v.y) : "memory");
+}
+__device__ __forceinline__ float2 ld_tw(const float2 *p) {
+  float2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double2 ld_tw(const double2 *p) {
+  double2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+
 // One tile per CTA. MODE 1: column pass (tile = tpc adjacent columns, staged
 // [e][p]); MODE 0: row pass (tile = tpc rows, staged [p][e]).
 template <typename T, int N, int FEAT, int MODE>
@@ -242,7 +262,7 @@ __device__ __forceinline__ void rr_butterflies(const fftz_pass_t &P, typename Cp
     const T2 *tw = (const T2 *)P.tw + P.tw_off[S];
     const int k = j & (NS - 1);
 #pragma unroll
-    for (int r = 1; r < 16; r++) v[r] = cmul(v[r], __ldg(tw + (r - 1) * NS + k));
+    for (int r = 1; r < 16; r++) v[r] = cmul(v[r], ld_tw(tw + (r - 1) * NS + k));
   }
   Dft<16>::template apply<T, T2>(v);
 }
@@ -336,8 +356,8 @@ __device__ __forceinline__ void tw4_parts(const fftz_pass_t &P, int64_t col, int
     h = r / L;
     l = r - h * L;
   }
-  hi = __ldg((const T2 *)P.tw4_hi + h);
-  lo = __ldg((const T2 *)P.tw4_lo + l);
+  hi = ld_tw((const T2 *)P.tw4_hi + h);
+  lo = ld_tw((const T2 *)P.tw4_lo + l);
 }
 
 // Last stage's outputs to HBM (lane map out_mode) with the pass epilogue. In
@@ -373,7 +393,7 @@ __device__ __forceinline__ void rr_store(const fftz_pass_t &P, const typename Cp
       if (r != 7 && r != 15) w = cmul(w, stp);
     }
     if (cj) y.y = -y.y;
-    ob[r * st] = y;
+    st_na(ob + r * st, y);
   }
 }
 
@@ -477,6 +497,258 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_rr_kernel(const __grid_
   }
 }
 
+// ------------------------------------------------------------- 16 x 256 split
+//
+// Persistent 4096-point float kernel, one CTA of 1024 threads per SM, tiles of
+// four transforms. The line is split as n = n0 + 16 m, k = k' + 256 k2:
+//   X[k' + 256 k2] = sum_n0 W16^{n0 k2} W4096^{n0 k'} Z_n0[k'],
+//   Z_n0[k'] = sum_m x[n0 + 16 m] W256^{m k'}.
+// The 64 sub-transforms Z_n0 of a tile (4 transforms x 16 n0) run one per
+// 16-lane group: each lane holds m = l + 16 s (s = 0..15), a radix-16 stage
+// over s, the W256 twiddle, a 16 x 16 transpose among the group's lanes and a
+// second radix-16 stage leave Z_n0[l + 16 k_hi] in lane l. One exchange across
+// the CTA then gives thread (transform p, k') its 16 values Z_n0[k'], and a
+// last radix-16 stage with the W4096 twiddle produces outputs k' + 256 r,
+// stored with the pass epilogue like the register-resident kernel's last
+// stage. Compared with three stages and two CTA-wide exchanges, the sub-
+// transforms need no CTA barrier: only the one exchange does (two rounds of
+// full complex values through a 64 KB buffer, half of the warps reading in
+// each round).
+//
+// Staging: the tile arrives as 16 TMA boxes (box s = elements [256 s, 256 s +
+// 256) of the four transforms), each box laid out [n0][m_l][transform] by the
+// tensor map's dimension order (column tiles, 32-byte swizzle) or
+// [transform][m_l][n0] (row tiles, 128-byte swizzle); a warp's groups read
+// their 16 values from one 256-byte slice of every box, bank-conflict-free.
+// The transpose of the sub-transforms reuses the warp's own slice (so it needs
+// no other buffer and no CTA barrier); the last warp to finish with its slice
+// issues the next tile's 16 boxes into the staging area. All index maps are
+// restated and checked on the CPU by tests/test_split_layouts.py.
+
+// staging, exchange, offsets, steps, mbarrier + counters; XM 1 adds the 32 KB stash
+constexpr int kSplitSmem = 16384 * 8 + 8192 * 8 + 16 * 8 + 16 * 8 + 16;
+constexpr int kSplitStash = 512 * 8 * 8;
+
+__device__ __forceinline__ void nb_sync(int id) { asm volatile("bar.sync %0, 1024;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ void nb_arrive(int id) { asm volatile("bar.arrive %0, 1024;" ::"r"(id) : "memory"); }
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(smem_addr(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Slice offset of the transpose slot for difference d = writer lane ^ reader
+// lane (XOR-linear in d): column tiles ([n0][m_l][col], 32-byte swizzle) and
+// row tiles ([row][m_l][n0], 128-byte swizzle).
+template <int MODE> __host__ __device__ constexpr int split_f(int d) {
+  return MODE == 1 ? (((d & 7) << 2) | (((d >> 2) & 1) << 1) | ((d >> 3) & 1))
+                   : (((d & 7) << 4) | ((d & 7) << 1) | ((d >> 3) & 1));
+}
+
+template <typename T, int N, int FEAT, int MODE, int OMODE, int XM>
+__global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_constant__ fftz_pass_t P,
+                                                                const __grid_constant__ CUtensorMap tmap,
+                                                                int64_t ntiles) {
+  static_assert(N == 4096 && sizeof(T) == 4, "4096-point float tiles");
+  typedef typename Cplx<T>::type T2;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *base = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
+  T2 *stg = (T2 *)base;                      // 16 boxes of 1024 complex
+  T2 *X = stg + 16384;                       // one exchange round: 8192 complex
+  int64_t *offs = (int64_t *)(X + 8192);     // 2 sets of {out[4], col[4]} by tile parity
+  T2 *steps = (T2 *)(offs + 16);             // 2 sets of {W^{256 col}[4], W^{2048 col}[4]}
+  uint64_t *bar = (uint64_t *)(steps + 16);
+  unsigned *cnt = (unsigned *)(bar + 1);      // warps done with the staging area (32 a tile)
+  volatile int *abort_flag = (volatile int *)(cnt + 1);
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int g = (lane >> 3) & 1, l = (lane & 7) | ((lane >> 4) << 3);
+  // the group's sub-transform (transform pw, subsequence n0w) and its slice
+  int pw, n0w, wb, c, rd0;
+  if (MODE == 1) {
+    const int a = w & 1;
+    n0w = w >> 1;
+    pw = 2 * a + g;
+    wb = n0w * 64;
+    c = (33 * g) ^ (2 * a);
+    rd0 = wb + ((l * 4 + 2 * ((l >> 2) & 1) + g) ^ (2 * a));
+  } else {
+    const int b = w & 7;
+    pw = w >> 3;
+    n0w = 2 * b + g;
+    wb = pw * 256;
+    c = (129 * g) ^ (2 * b);
+    rd0 = wb + ((l * 16 + 2 * (l & 7) + g) ^ (2 * b));
+  }
+  const int u = split_f<MODE>(l) ^ c;
+  const int xw = (pw * 16 + n0w) * 128 + (l ^ (4 * ((pw >> 1) & 1) + 8 * ((pw ^ n0w) & 1)));
+  // exchange reader: thread (pr, kr) of the output lane map
+  const int pr = OMODE == 1 ? (tid & 3) : (tid >> 8);
+  const int kr = OMODE == 1 ? (tid >> 2) : (tid & 255);
+  const int rround = kr >> 7, kl = kr & 127;
+  const int xr_e = pr * 2048 + (kl ^ (4 * ((pr >> 1) & 1) + 8 * (pr & 1)));
+  const int xr_o = pr * 2048 + (kl ^ (4 * ((pr >> 1) & 1) + 8 * ((pr & 1) ^ 1)));
+  // one-component layout: float (p * 16 + n0) * 256 + (k' ^ S), S = 8 (p >> 1 & 1) + 16 ((p ^ n0) & 1);
+  // writers take even/odd k_hi bases, readers even/odd n0 bases
+  const int sw1 = 8 * ((pw >> 1) & 1) + 16 * ((pw ^ n0w) & 1);
+  const int xfw = (pw * 16 + n0w) * 256 + (l ^ (sw1 & 15)), s4 = 16 * (sw1 >> 4);
+  const int xfw_e = xfw + s4, xfw_o = xfw - s4;
+  const int xfr_e = pr * 4096 + (kr ^ (8 * ((pr >> 1) & 1) + 16 * (pr & 1)));
+  const int xfr_o = pr * 4096 + (kr ^ (8 * ((pr >> 1) & 1) + 16 * ((pr & 1) ^ 1)));
+  // stash slot of a round-1 reader (XM 1): 512 threads, [value][thread]
+  const int si = OMODE == 1 ? (tid & 511) : ((w >> 3) * 128 + (w & 3) * 32 + lane);
+  const int64_t b0 = P.bdim[0];
+  const T2 *tw1 = (const T2 *)P.tw + P.tw_off[1];
+  const T2 *tw2 = (const T2 *)P.tw + P.tw_off[2];
+  const bool cjin = (P.flags & FFTZ_F_CONJ_IN) != 0;
+  auto issue = [&](int64_t tile) {
+    const int64_t tf0 = tile * 4;
+    const int c0 = (int)(tf0 % b0);
+    const int z = (int)(tf0 / b0);
+    mbar_expect_tx(bar, (unsigned)(N * 4 * sizeof(T2)));
+#pragma unroll 1
+    for (int s = 0; s < 16; s++) {
+      if (MODE == 1)
+        tma_load_4d(stg + s * 1024, &tmap, c0, 16 * s, 0, z, bar);
+      else
+        tma_load_4d(stg + s * 1024, &tmap, 0, 16 * s, c0, z, bar);
+    }
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    *cnt = 0;
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  int64_t tile = blockIdx.x;
+  if (tid == 0 && tile < ntiles) issue(tile);
+  unsigned it = 0;
+  for (; tile < ntiles; it++, tile += gridDim.x) {
+    int64_t *s_out = offs + (size_t)(it & 1u) * 8;
+    int64_t *s_col = s_out + 4;
+    T2 *s_stp = steps + (size_t)(it & 1u) * 8;
+    if (tid < 4) {
+      int64_t io;
+      batch_offsets(P, tile * 4 + tid, &io, s_out + tid, s_col + tid);
+      if constexpr ((FEAT & FEAT_TW4) != 0) {
+        s_stp[tid] = tw4<T>(P, s_col[tid], N / 16);
+        s_stp[4 + tid] = tw4<T>(P, s_col[tid], N / 2);
+      }
+    }
+    // bounded wait for the staged tile; a wait that gives up flags the
+    // failure for the host and stops further copies (the CTA still passes
+    // every barrier, computing on whatever the staging area holds)
+    if (!*abort_flag) {
+      bool ok = false;
+      for (long i = 0; i < (1L << 22); i++)
+        if (mbar_try_wait(bar, it & 1u)) {
+          ok = true;
+          break;
+        }
+      if (!ok) {
+        *abort_flag = (int)it + 1;
+        if (lane == 0) atomicExch(&g_tma_wait_failed, 1);
+      }
+    }
+    T2 v[16];
+#pragma unroll
+    for (int s = 0; s < 16; s++) {
+      T2 x = stg[s * 1024 + rd0];
+      if (cjin) x.y = -x.y;
+      v[s] = x;
+    }
+    Dft<16>::template apply<T, T2>(v);
+#pragma unroll
+    for (int k = 1; k < 16; k++) v[k] = cmul(v[k], ld_tw(tw1 + (k - 1) * 16 + l));
+    __syncwarp();  // every lane of the warp has read its staged values
+    {
+      T2 *wbase = stg + l * 1024 + wb;
+#pragma unroll
+      for (int k = 0; k < 16; k++) wbase[u ^ split_f<MODE>(k)] = v[k];
+      __syncwarp();
+#pragma unroll
+      for (int x = 0; x < 16; x++) v[x] = stg[x * 1024 + wb + (u ^ split_f<MODE>(x))];
+    }
+    Dft<16>::template apply<T, T2>(v);  // lane l now holds Z[l + 16 k_hi], k_hi = 0..15
+    // release the slice; the last warp issues the next tile's copies
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      const unsigned old = atomicAdd(cnt, 1u);
+      if ((old & 31u) == 31u && tile + gridDim.x < ntiles && !*abort_flag) {
+        __threadfence_block();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(tile + gridDim.x);
+      }
+    }
+    T2 y[16];
+    if constexpr (XM == 0) {
+      // exchange of one real component at a time (x parts, then y parts)
+      // through X viewed as 16384 floats: no thread holds more than 16
+      // complex values at once
+      T *Xf = (T *)X;
+      nb_sync(4);  // the previous tile's readers are done with X
+#pragma unroll
+      for (int k = 0; k < 16; k++) Xf[((k & 1) ? xfw_o : xfw_e) + 16 * k] = v[k].x;
+      nb_sync(1);
+#pragma unroll
+      for (int n0 = 0; n0 < 16; n0++) y[n0].x = Xf[((n0 & 1) ? xfr_o : xfr_e) + n0 * 256];
+      nb_sync(2);
+#pragma unroll
+      for (int k = 0; k < 16; k++) Xf[((k & 1) ? xfw_o : xfw_e) + 16 * k] = v[k].y;
+      nb_sync(3);
+#pragma unroll
+      for (int n0 = 0; n0 < 16; n0++) y[n0].y = Xf[((n0 & 1) ? xfr_o : xfr_e) + n0 * 256];
+    } else {
+      // two rounds of full complex values: round 1 k' < 128 (k_hi < 8),
+      // round 2 the rest; the round-1 readers keep their round-2 values in
+      // a stash instead of registers while they read
+      T2 *stash = (T2 *)(abort_flag + 1) + si;
+      nb_sync(4);  // the previous tile's round-2 readers are done with X
+#pragma unroll
+      for (int kh = 0; kh < 8; kh++) X[xw + 16 * kh] = v[kh];
+      if (rround == 0) {
+#pragma unroll
+        for (int kh = 0; kh < 8; kh++) stash[kh * 512] = v[8 + kh];
+        nb_sync(1);
+#pragma unroll
+        for (int n0 = 0; n0 < 16; n0++) y[n0] = X[((n0 & 1) ? xr_o : xr_e) + n0 * 128];
+        nb_sync(2);  // round-1 reads done
+#pragma unroll
+        for (int kh = 0; kh < 8; kh++) X[xw + 16 * kh] = stash[kh * 512];
+        nb_arrive(3);
+      } else {
+        nb_arrive(1);
+        nb_sync(2);
+#pragma unroll
+        for (int kh = 0; kh < 8; kh++) X[xw + 16 * kh] = v[8 + kh];
+        nb_sync(3);
+#pragma unroll
+        for (int n0 = 0; n0 < 16; n0++) y[n0] = X[((n0 & 1) ? xr_o : xr_e) + n0 * 128];
+      }
+    }
+    T2 hi = zero2<T2>(), lo = zero2<T2>();
+    if constexpr ((FEAT & FEAT_TW4) != 0) tw4_parts<T>(P, s_col[pr], kr, hi, lo);
+#pragma unroll
+    for (int n0 = 1; n0 < 16; n0++) y[n0] = cmul(y[n0], ld_tw(tw2 + (n0 - 1) * 256 + kr));
+    Dft<16>::template apply<T, T2>(y);
+    rr_store<T, N, 2, FEAT>(P, y, kr, s_out[pr], s_col[pr], hi, lo, s_stp[pr], s_stp[4 + pr]);
+  }
+  // after a wait that gave up, give copies still in flight a bounded time to
+  // land before the CTA's shared memory is released
+  const int af = *abort_flag;
+  if (af && tid == 0) {
+    for (long i = 0; i < (1L << 22); i++)
+      if (mbar_try_wait(bar, (unsigned)(af - 1) & 1u)) break;
+  }
+}
+
 }  // namespace fftz
 
 // ------------------------------------------------------------------- host
@@ -542,6 +814,95 @@ const void *tma_rr_kernel(int dtype, int n, int tw4, int mode) {
 }
 
 
+template <int XM> const void *split_pick(int tw4, int mode, int omode) {
+  using fftz::fft_tma_split_kernel;
+  if (tw4)
+    return mode ? (omode ? (const void *)&fft_tma_split_kernel<float, 4096, 1, 1, 1, XM>
+                         : (const void *)&fft_tma_split_kernel<float, 4096, 1, 1, 0, XM>)
+                : (omode ? (const void *)&fft_tma_split_kernel<float, 4096, 1, 0, 1, XM>
+                         : (const void *)&fft_tma_split_kernel<float, 4096, 1, 0, 0, XM>);
+  return mode ? (omode ? (const void *)&fft_tma_split_kernel<float, 4096, 0, 1, 1, XM>
+                       : (const void *)&fft_tma_split_kernel<float, 4096, 0, 1, 0, XM>)
+              : (omode ? (const void *)&fft_tma_split_kernel<float, 4096, 0, 0, 1, XM>
+                       : (const void *)&fft_tma_split_kernel<float, 4096, 0, 0, 0, XM>);
+}
+
+/* Launches a 4096-point float pass through the 16 x 256 split kernel; -1
+ * (nothing launched) when the pass or its buffers do not qualify. */
+int launch_split(const fftz_pass_t *p, void *stream) {
+  if (p->n != 4096 || p->dtype != 0 || p->tpc != 4 || p->tpt != 256) return -1;
+  if (p->variant != FFTZ_VAR_FAST && p->variant != FFTZ_VAR_FAST_TW4) return -1;
+  if (p->in_kind != FFTZ_IN_COMPLEX || p->out_kind != FFTZ_OUT_COMPLEX) return -1;
+  if ((p->flags & ~(FFTZ_F_CONJ_IN | FFTZ_F_CONJ_OUT | FFTZ_F_TW4)) != 0) return -1;
+  if (p->nbdims < 1 || p->nbdims > 2 || p->ind_in || p->ind_out) return -1;
+  const int64_t b0 = p->bdim[0], b1 = p->nbdims == 2 ? p->bdim[1] : 1;
+  if (b0 % 4 || p->ntf != b0 * b1 || b0 > 0x7fffffff || b1 > 0x7fffffff) return -1;
+  if (((uintptr_t)p->in & 15) != 0 || !encoder()) return -1;
+  const int mode = p->in_mode, omode = p->out_mode;
+  cuuint64_t dims[4], strides[3];
+  cuuint32_t box[4], estr[4] = {1, 1, 1, 1};
+  CUtensorMapSwizzle swz;
+  if (mode == 1) {
+    /* element e = n0 + 16 m of column c: dims (c, m, n0, outer batch) */
+    if (p->ibs[0] != 1 || p->ies <= 0) return -1;
+    dims[0] = (cuuint64_t)b0;
+    dims[1] = 256;
+    dims[2] = 16;
+    strides[0] = (cuuint64_t)(16 * p->ies * 8);
+    strides[1] = (cuuint64_t)(p->ies * 8);
+    box[0] = 4;
+    box[1] = 16;
+    box[2] = 16;
+    swz = CU_TENSOR_MAP_SWIZZLE_32B;
+  } else {
+    /* element e = n0 + 16 m of row r: dims (n0, m, r, outer batch) */
+    if (p->ies != 1 || p->ibs[0] <= 0) return -1;
+    dims[0] = 16;
+    dims[1] = 256;
+    dims[2] = (cuuint64_t)b0;
+    strides[0] = 128;
+    strides[1] = (cuuint64_t)(p->ibs[0] * 8);
+    box[0] = 16;
+    box[1] = 16;
+    box[2] = 4;
+    swz = CU_TENSOR_MAP_SWIZZLE_128B;
+  }
+  dims[3] = (cuuint64_t)b1;
+  box[3] = 1;
+  strides[2] = p->nbdims == 2 ? (cuuint64_t)(p->ibs[1] * 8) : (cuuint64_t)(4096 * 8 * (mode == 1 ? p->ies : 1));
+  if (p->nbdims == 2 && p->ibs[1] <= 0) return -1;
+  for (int i = 0; i < 3; i++)
+    if (strides[i] % 16 || strides[i] >= (1ULL << 40)) return -1;
+  CUtensorMap map;
+  if (g_encode(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, (void *)p->in, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return -1;
+  const int xm = p->use_tma == 5;
+  const int tw4 = p->variant == FFTZ_VAR_FAST_TW4;
+  const void *fn = xm ? split_pick<1>(tw4, mode, omode) : split_pick<0>(tw4, mode, omode);
+  const size_t smem = (size_t)fftz::kSplitSmem + (xm ? fftz::kSplitStash : 0) + 1024;
+  static const void *opted[64][16];
+  static int nopted[64], nsm[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  int seen = 0;
+  for (int i = 0; i < nopted[dev]; i++)
+    if (opted[dev][i] == fn) seen = 1;
+  if (!seen) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    if (nopted[dev] < 16) opted[dev][nopted[dev]++] = fn;
+  }
+  if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+  int64_t ntiles = p->ntf / 4;
+  const int64_t cap = nsm[dev] > 0 ? nsm[dev] : 148;
+  const dim3 grid((unsigned)(ntiles < cap ? ntiles : cap)), block(1024);
+  void *args[3] = {(void *)p, (void *)&map, (void *)&ntiles};
+  return (int)cudaLaunchKernel(fn, grid, block, args, smem, (cudaStream_t)stream);
+}
+
 const void *tma_kernel(int dtype, int n, int tw4, int mode) {
   if (dtype == 0)
     return tw4 ? (mode ? pick<float, 1, 1>(n) : pick<float, 1, 0>(n))
@@ -564,8 +925,12 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   const int64_t b0 = p->bdim[0], b1 = p->nbdims == 2 ? p->bdim[1] : 1;
   if (p->tpc < 1 || b0 % p->tpc || p->ntf != b0 * b1) return -1;
   if (((uintptr_t)p->in & 15) != 0) return -1;
+  if (p->use_tma == 4 || p->use_tma == 5) {
+    const int e = launch_split(p, stream);
+    if (e >= 0) return e;
+  }
   const int tw4 = p->variant == FFTZ_VAR_FAST_TW4;
-  int rr = p->use_tma == 3 && p->tpc * p->tpt <= 1024;
+  int rr = p->use_tma >= 3 && p->tpc * p->tpt <= 1024;
   const void *fn = rr ? tma_rr_kernel(p->dtype, p->n, tw4, mode) : nullptr;
   if (!fn) rr = 0;
   int pipe = !rr && p->use_tma == 2;

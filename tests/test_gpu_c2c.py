@@ -231,3 +231,30 @@ def test_shared_memory_twiddles(dtype, n, batch):
     finally:
         lib.aoclfftz_gpu_set_hints(None)
 
+
+
+@pytest.mark.parametrize("family,tag", [(9, "tma-split"), (10, "tma-split2")])
+@pytest.mark.parametrize("n,batch,want", [(1 << 24, 1, 2), (1 << 24, 2, 2), (1 << 23, 2, 1), (4096, 64, 1),
+                                          (4096, 1001, 0), (1 << 20, 3, 0)])
+def test_split_tiles(family, tag, n, batch, want):
+    """Kernel families 9 and 10: 4096-point float passes as 16 x 256 split
+    tiles (persistent CTAs, the 64 sub-transforms of a tile in 16-lane groups,
+    one exchange across the CTA; 9 exchanges one real component at a time, 10
+    full complex values in two rounds). Four-step 2^24 runs both passes that
+    way (column tiles with the four-step twiddle, row tiles with the
+    transposed store), 2^23 its 4096-point column pass, plain 4096-point rows
+    as row tiles with row stores; 1001 rows do not form whole tiles and take
+    the register-resident kernel; 2^20 does not qualify. Against the oracle,
+    both directions."""
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi
+    lib = aoclfftz_b200.load()
+    h = abi.Hints()
+    h.kernel_family = family
+    lib.aoclfftz_gpu_set_hints(C.byref(h))
+    try:
+        for d in (0, 1):
+            _, plan = check_c2c("f32", [(n, 1, 1)], [(batch, n, n)], d, compare_ref=n < (1 << 20))
+            assert plan.count(tag + "]") == want, plan
+    finally:
+        lib.aoclfftz_gpu_set_hints(None)

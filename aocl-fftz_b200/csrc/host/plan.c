@@ -286,8 +286,8 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
          * round) or 10 (full complex values in two rounds, round-1 readers'
          * values stashed in shared memory: 0.326 / 0.282 ms) */
         if ((k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4) && pl->dtype == 0 && n == 4096 &&
-            (fam == 9 || fam == 10 || (fam == 0 && (k->in_mode == 1 || k->out_mode == 1))))
-            k->use_tma = fam == 10 ? 5 : 4;
+            (fam == 9 || fam == 10 || fam == 11 || (fam == 0 && (k->in_mode == 1 || k->out_mode == 1))))
+            k->use_tma = fam == 10 ? 5 : fam == 11 ? 6 : 4;
         /* stage twiddles copied to shared memory by each CTA (hint twiddles = 2) */
         k->smem_tw = pl->hints.twiddles == 2 && !ragged_mode(pl) && n >= 512;
         if ((tw4 || tabs) && n < 32 && !(variant_bits & 4))

@@ -549,6 +549,32 @@ template <int MODE> __host__ __device__ constexpr int split_f(int d) {
                    : (((d & 7) << 4) | ((d & 7) << 1) | ((d >> 3) & 1));
 }
 
+// Tensor-memory stash (XM 2): a warp's 32 lanes keep 16 words each in their
+// own TMEM lanes (the warp's lane quarter), 16 columns per warp.
+__device__ __forceinline__ void tm_st16(uint32_t taddr, const float2 (&v)[8]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0].x)), "r"(__float_as_uint(v[0].y)), "r"(__float_as_uint(v[1].x)),
+      "r"(__float_as_uint(v[1].y)), "r"(__float_as_uint(v[2].x)), "r"(__float_as_uint(v[2].y)),
+      "r"(__float_as_uint(v[3].x)), "r"(__float_as_uint(v[3].y)), "r"(__float_as_uint(v[4].x)),
+      "r"(__float_as_uint(v[4].y)), "r"(__float_as_uint(v[5].x)), "r"(__float_as_uint(v[5].y)),
+      "r"(__float_as_uint(v[6].x)), "r"(__float_as_uint(v[6].y)), "r"(__float_as_uint(v[7].x)),
+      "r"(__float_as_uint(v[7].y))
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tm_ld8(uint32_t taddr, float2 (&v)[4]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr)
+               : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 4; i++) v[i] = make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+}
+
 template <typename T, int N, int FEAT, int MODE, int OMODE, int XM>
 __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_constant__ fftz_pass_t P,
                                                                 const __grid_constant__ CUtensorMap tmap,
@@ -617,6 +643,7 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
         tma_load_4d(stg + s * 1024, &tmap, 0, 16 * s, c0, z, bar);
     }
   };
+  uint32_t *s_taddr = (uint32_t *)(abort_flag + 1);
   if (tid == 0) {
     mbar_init(bar, 1);
     *cnt = 0;
@@ -624,7 +651,18 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
+  if (XM == 2 && w == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_addr(s_taddr))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (XM == 2) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  if (XM == 2) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // this warp's stash columns (round-1 reader warps, four per lane quarter)
+  const uint32_t tstash = XM == 2 ? *s_taddr + ((uint32_t)(32 * (w & 3)) << 16) +
+                                        (uint32_t)(16 * (OMODE == 1 ? (w >> 2) : (w >> 3)))
+                                  : 0u;
   int64_t tile = blockIdx.x;
   if (tid == 0 && tile < ntiles) issue(tile);
   unsigned it = 0;
@@ -714,14 +752,31 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
 #pragma unroll
       for (int kh = 0; kh < 8; kh++) X[xw + 16 * kh] = v[kh];
       if (rround == 0) {
+        if constexpr (XM == 2) {
+          T2 hv[8];
 #pragma unroll
-        for (int kh = 0; kh < 8; kh++) stash[kh * 512] = v[8 + kh];
+          for (int kh = 0; kh < 8; kh++) hv[kh] = v[8 + kh];
+          tm_st16(tstash, hv);
+        } else {
+#pragma unroll
+          for (int kh = 0; kh < 8; kh++) stash[kh * 512] = v[8 + kh];
+        }
         nb_sync(1);
 #pragma unroll
         for (int n0 = 0; n0 < 16; n0++) y[n0] = X[((n0 & 1) ? xr_o : xr_e) + n0 * 128];
         nb_sync(2);  // round-1 reads done
+        if constexpr (XM == 2) {
 #pragma unroll
-        for (int kh = 0; kh < 8; kh++) X[xw + 16 * kh] = stash[kh * 512];
+          for (int hq = 0; hq < 2; hq++) {
+            T2 hv[4];
+            tm_ld8(tstash + 8 * hq, hv);
+#pragma unroll
+            for (int kh = 0; kh < 4; kh++) X[xw + 16 * (4 * hq + kh)] = hv[kh];
+          }
+        } else {
+#pragma unroll
+          for (int kh = 0; kh < 8; kh++) X[xw + 16 * kh] = stash[kh * 512];
+        }
         nb_arrive(3);
       } else {
         nb_arrive(1);
@@ -746,6 +801,14 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
   if (af && tid == 0) {
     for (long i = 0; i < (1L << 22); i++)
       if (mbar_try_wait(bar, (unsigned)(af - 1) & 1u)) break;
+  }
+  if constexpr (XM == 2) {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (w == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(*s_taddr) : "memory");
+    }
   }
 }
 
@@ -878,11 +941,13 @@ int launch_split(const fftz_pass_t *p, void *stream) {
                CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return -1;
-  const int xm = p->use_tma == 5;
+  const int xm = p->use_tma == 5 ? 1 : p->use_tma == 6 ? 2 : 0;
   const int tw4 = p->variant == FFTZ_VAR_FAST_TW4;
-  const void *fn = xm ? split_pick<1>(tw4, mode, omode) : split_pick<0>(tw4, mode, omode);
-  const size_t smem = (size_t)fftz::kSplitSmem + (xm ? fftz::kSplitStash : 0) + 1024;
-  static const void *opted[64][16];
+  const void *fn = xm == 1 ? split_pick<1>(tw4, mode, omode)
+                 : xm == 2 ? split_pick<2>(tw4, mode, omode)
+                           : split_pick<0>(tw4, mode, omode);
+  const size_t smem = (size_t)fftz::kSplitSmem + (xm == 1 ? fftz::kSplitStash : 16) + 1024;
+  static const void *opted[64][32];
   static int nopted[64], nsm[64];
   int dev = 0;
   cudaGetDevice(&dev);
@@ -893,7 +958,7 @@ int launch_split(const fftz_pass_t *p, void *stream) {
   if (!seen) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
-    if (nopted[dev] < 16) opted[dev][nopted[dev]++] = fn;
+    if (nopted[dev] < 32) opted[dev][nopted[dev]++] = fn;
   }
   if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
   int64_t ntiles = p->ntf / 4;
@@ -925,7 +990,7 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   const int64_t b0 = p->bdim[0], b1 = p->nbdims == 2 ? p->bdim[1] : 1;
   if (p->tpc < 1 || b0 % p->tpc || p->ntf != b0 * b1) return -1;
   if (((uintptr_t)p->in & 15) != 0) return -1;
-  if (p->use_tma == 4 || p->use_tma == 5) {
+  if (p->use_tma >= 4) {
     const int e = launch_split(p, stream);
     if (e >= 0) return e;
   }

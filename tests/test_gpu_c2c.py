@@ -233,14 +233,15 @@ def test_shared_memory_twiddles(dtype, n, batch):
 
 
 
-@pytest.mark.parametrize("family,tag", [(9, "tma-split"), (10, "tma-split2")])
+@pytest.mark.parametrize("family,tag", [(9, "tma-split"), (10, "tma-split2"), (11, "tma-split3")])
 @pytest.mark.parametrize("n,batch,want", [(1 << 24, 1, 2), (1 << 24, 2, 2), (1 << 23, 2, 1), (4096, 64, 1),
                                           (4096, 1001, 0), (1 << 20, 3, 0)])
 def test_split_tiles(family, tag, n, batch, want):
     """Kernel families 9 and 10: 4096-point float passes as 16 x 256 split
     tiles (persistent CTAs, the 64 sub-transforms of a tile in 16-lane groups,
     one exchange across the CTA; 9 exchanges one real component at a time, 10
-    full complex values in two rounds). Four-step 2^24 runs both passes that
+    full complex values in two rounds with a shared-memory stash, 11 the same
+    with the stash in tensor memory). Four-step 2^24 runs both passes that
     way (column tiles with the four-step twiddle, row tiles with the
     transposed store), 2^23 its 4096-point column pass, plain 4096-point rows
     as row tiles with row stores; 1001 rows do not form whole tiles and take

@@ -53,6 +53,44 @@ void fz_log(const fz_plan *pl, const char *fmt, ...)
 
 const FFTZ_CHAR *aoclfftz_gpu_last_error(FFTZ_VOID) { return g_err; }
 
+int64_t fz_inj_tma_short = 0, fz_inj_ragged_wait = 0, fz_inj_ragged_dep = 0, fz_inj_alloc_fail = 0;
+
+int fz_dev_malloc(void **p, size_t bytes)
+{
+    if (__atomic_load_n(&fz_inj_alloc_fail, __ATOMIC_ACQUIRE) > 0 &&
+        __atomic_sub_fetch(&fz_inj_alloc_fail, 1, __ATOMIC_ACQ_REL) >= 0)
+    {
+        *p = NULL;
+        return -1;
+    }
+    if (cudaMalloc(p, bytes) != cudaSuccess)
+    {
+        cudaGetLastError();
+        *p = NULL;
+        return -1;
+    }
+    return 0;
+}
+
+FFTZ_INT32 aoclfftz_gpu_inject_fault(FFTZ_INT32 kind, FFTZ_INT64 value)
+{
+    if (value < 0) return -1;
+    switch (kind)
+    {
+    case AOCLFFTZ_GPU_FAULT_NONE:
+        fz_inj_tma_short = fz_inj_ragged_wait = fz_inj_ragged_dep = fz_inj_alloc_fail = 0;
+        return 0;
+    case AOCLFFTZ_GPU_FAULT_TMA_SHORT:
+        if (value > (1 << 20)) return -1;
+        fz_inj_tma_short = value;
+        return 0;
+    case AOCLFFTZ_GPU_FAULT_RAGGED_WAIT: fz_inj_ragged_wait = value; return 0;
+    case AOCLFFTZ_GPU_FAULT_RAGGED_DEP: fz_inj_ragged_dep = value; return 0;
+    case AOCLFFTZ_GPU_FAULT_ALLOC: __atomic_store_n(&fz_inj_alloc_fail, value, __ATOMIC_RELEASE); return 0;
+    }
+    return -1;
+}
+
 /* ------------------------------------------------------------- validation */
 
 typedef struct
@@ -215,7 +253,7 @@ static void *setup_impl(fz_desc *d, int dtype)
     /* device tables: one allocation, then every pass's pointers */
     if (pl->blob.len)
     {
-        if (cudaMalloc(&pl->dtab, pl->blob.len) != cudaSuccess ||
+        if (fz_dev_malloc(&pl->dtab, pl->blob.len) ||
             cudaMemcpy(pl->dtab, pl->blob.p, pl->blob.len, cudaMemcpyHostToDevice) != cudaSuccess)
         {
             cudaGetLastError();
@@ -242,7 +280,7 @@ static void *setup_impl(fz_desc *d, int dtype)
     pl->scratch_bytes = 0;
     for (int i = 0; i < pl->nscratch; i++)
         pl->scratch_bytes += (pl->scratch_elems[i] * csz + 255) & ~(int64_t)255;
-    if (pl->scratch_bytes > 0 && cudaMalloc(&pl->scratch, (size_t)pl->scratch_bytes) != cudaSuccess)
+    if (pl->scratch_bytes > 0 && fz_dev_malloc(&pl->scratch, (size_t)pl->scratch_bytes))
     {
         cudaGetLastError();
         fz_set_error("device allocation of %lld scratch bytes failed", (long long)pl->scratch_bytes);
@@ -456,7 +494,7 @@ static int prepare_chunks(fz_plan *pl)
     pl->pipe_out_bytes = pl->placement == 0 ? 0 : (ch->out_bytes + 255) & ~(int64_t)255;
     if (pl->placement == 0 && ch->out_bytes > ch->in_bytes) pl->pipe_in_bytes = (ch->out_bytes + 255) & ~(int64_t)255;
     pl->pipe_slot_bytes = pl->pipe_in_bytes + pl->pipe_out_bytes + ((ch->scratch_bytes + 255) & ~(int64_t)255);
-    if (cudaMalloc(&pl->pipe_buf, (size_t)(3 * pl->pipe_slot_bytes)) != cudaSuccess)
+    if (fz_dev_malloc(&pl->pipe_buf, (size_t)(3 * pl->pipe_slot_bytes)))
     {
         cudaGetLastError();
         return -1;
@@ -537,12 +575,23 @@ static aoclfftz_error_type run_pipelined(fz_plan *pl, void *in, void *out)
     return AOCLFFTZ_SUCCESS;
 }
 
+static aoclfftz_error_type run_on_device(fz_plan *pl, void *in, void *out);
+
+/* Executes on the plan's device and restores the caller's current device. */
 static aoclfftz_error_type run(fz_plan *pl, void *in, void *out)
 {
     if (pl->nop) return AOCLFFTZ_SUCCESS;
     int cur = -1;
     cudaGetDevice(&cur);
-    if (cur != pl->device) cudaSetDevice(pl->device);
+    const int sw = cur != pl->device;
+    if (sw) cudaSetDevice(pl->device);
+    aoclfftz_error_type r = run_on_device(pl, in, out);
+    if (sw && cur >= 0) cudaSetDevice(cur);
+    return r;
+}
+
+static aoclfftz_error_type run_on_device(fz_plan *pl, void *in, void *out)
+{
     cudaStream_t st = (cudaStream_t)pl->stream;
     const int in_dev = device_usable(in);
     const int out_dev = device_usable(out);
@@ -581,7 +630,7 @@ static aoclfftz_error_type run(fz_plan *pl, void *in, void *out)
             if (pl->stage) cudaFree(pl->stage);
             pl->stage = NULL;
             pl->stage_bytes = 0;
-            if (cudaMalloc(&pl->stage, (size_t)stage_need) != cudaSuccess)
+            if (fz_dev_malloc(&pl->stage, (size_t)stage_need))
             {
                 cudaGetLastError();
                 fz_set_error("staging allocation of %lld bytes failed", (long long)stage_need);
@@ -650,6 +699,7 @@ static aoclfftz_error_type run(fz_plan *pl, void *in, void *out)
             fftz_pass_t k = pl->pass[i].k;
             k.in = (const unsigned char *)buf[pl->pass[i].src] + pl->pass[i].in_off;
             k.out = (unsigned char *)buf[pl->pass[i].dst] + pl->pass[i].out_off;
+            k.test_tx_short = (int32_t)fz_inj_tma_short;
             e = fftz_launch_pass(&k, st);
         }
         if (ev) cudaEventRecord(ev[1], st);
@@ -759,7 +809,8 @@ aoclfftz_error_type aoclfftz_gpu_synchronize(FFTZ_VOID *handle)
         {
             if (fftz_tma_wait_failed())
             {
-                fz_set_error("a TMA-fed pass gave up waiting for its tile copies (results invalid)");
+                fz_set_error("a TMA-fed pass gave up waiting for its tile copies (its results, and those of "
+                             "later work on the same stream, are invalid)");
                 return AOCLFFTZ_EXECUTION_FAILURE;
             }
             break;
@@ -769,6 +820,8 @@ aoclfftz_error_type aoclfftz_gpu_synchronize(FFTZ_VOID *handle)
         int flag = 0;
         if (cudaMemcpy(&flag, pl->rg->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess || flag)
         {
+            /* reported once: later runs on the handle start with a clear flag */
+            if (flag) cudaMemset(pl->rg->d_err, 0, sizeof(int));
             fz_set_error("ragged executor: a dependency wait gave up (results invalid)");
             return AOCLFFTZ_EXECUTION_FAILURE;
         }

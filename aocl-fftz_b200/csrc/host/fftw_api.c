@@ -145,13 +145,23 @@ static void fw_real_side(int rank, const int *n, int stride, int half, int inpla
 
 static int g_nthreads = 1;
 
+/* FFTW defines only FFTW_FORWARD (-1) and FFTW_BACKWARD (+1): 0 / 1 for the
+ * planner's direction, -1 (no plan) for any other sign */
+static int fw_sign(int sign)
+{
+    if (sign == FFTW_FORWARD) return 0;
+    if (sign == FFTW_BACKWARD) return 1;
+    fz_set_error("FFTW sign %d is neither FFTW_FORWARD (-1) nor FFTW_BACKWARD (+1)", sign);
+    return -1;
+}
+
 #define FW_DEFINE(P, DT, R, Cx)                                                                                       \
     P##_plan P##_plan_dft(int rank, const int *n, Cx *in, Cx *out, int sign, unsigned flags)                          \
     {                                                                                                                  \
         fw_dim d[16];                                                                                                  \
         (void)flags;                                                                                                   \
-        if (fw_dense(rank, n, d)) return NULL;                                                                         \
-        return fw_make(DT, 0, sign == FFTW_FORWARD ? 0 : 1, rank, d, 0, NULL, in, out);                              \
+        if (fw_sign(sign) < 0 || fw_dense(rank, n, d)) return NULL;                                                    \
+        return fw_make(DT, 0, fw_sign(sign), rank, d, 0, NULL, in, out);                              \
     }                                                                                                                  \
     P##_plan P##_plan_dft_1d(int n, Cx *in, Cx *out, int sign, unsigned flags)                                        \
     {                                                                                                                  \
@@ -173,21 +183,22 @@ static int g_nthreads = 1;
     {                                                                                                                  \
         fw_dim d[16], h;                                                                                               \
         (void)flags;                                                                                                   \
-        if (rank < 0 || rank > 16 || (rank > 0 && !n)) return NULL;                                                    \
+        if (rank < 0 || rank > 16 || (rank > 0 && !n) || fw_sign(sign) < 0) return NULL;                              \
         for (int i = 0; i < rank; i++) d[i].n = n[i];                                                                  \
         fw_many_side(rank, n, inembed, istride, d, 1);                                                                 \
         fw_many_side(rank, n, onembed, ostride, d, 0);                                                                 \
         h.n = howmany;                                                                                                 \
         h.is = idist;                                                                                                  \
         h.os = odist;                                                                                                  \
-        return fw_make(DT, 0, sign == FFTW_FORWARD ? 0 : 1, rank, d, 1, &h, in, out);                                \
+        return fw_make(DT, 0, fw_sign(sign), rank, d, 1, &h, in, out);                                \
     }                                                                                                                  \
     P##_plan P##_plan_guru64_dft(int rank, const P##_iodim64 *dims, int hr, const P##_iodim64 *hd, Cx *in, Cx *out,   \
                                  int sign, unsigned flags)                                                             \
     {                                                                                                                  \
         fw_dim d[16], h[16];                                                                                           \
         (void)flags;                                                                                                   \
-        if (rank < 0 || rank > 16 || hr < 0 || hr > 16 || (rank && !dims) || (hr && !hd)) return NULL;                \
+        if (rank < 0 || rank > 16 || hr < 0 || hr > 16 || (rank && !dims) || (hr && !hd) || fw_sign(sign) < 0)       \
+            return NULL;                                                                                               \
         for (int i = 0; i < rank; i++)                                                                                 \
         {                                                                                                              \
             d[i].n = dims[i].n;                                                                                        \
@@ -200,13 +211,14 @@ static int g_nthreads = 1;
             h[i].is = hd[i].is;                                                                                        \
             h[i].os = hd[i].os;                                                                                        \
         }                                                                                                              \
-        return fw_make(DT, 0, sign == FFTW_FORWARD ? 0 : 1, rank, d, hr, h, in, out);                                \
+        return fw_make(DT, 0, fw_sign(sign), rank, d, hr, h, in, out);                                \
     }                                                                                                                  \
     P##_plan P##_plan_guru_dft(int rank, const P##_iodim *dims, int hr, const P##_iodim *hd, Cx *in, Cx *out,         \
                                int sign, unsigned flags)                                                               \
     {                                                                                                                  \
         P##_iodim64 d[16], h[16];                                                                                      \
-        if (rank < 0 || rank > 16 || hr < 0 || hr > 16 || (rank && !dims) || (hr && !hd)) return NULL;                \
+        if (rank < 0 || rank > 16 || hr < 0 || hr > 16 || (rank && !dims) || (hr && !hd) || fw_sign(sign) < 0)       \
+            return NULL;                                                                                               \
         for (int i = 0; i < rank; i++)                                                                                 \
         {                                                                                                              \
             d[i].n = dims[i].n;                                                                                        \

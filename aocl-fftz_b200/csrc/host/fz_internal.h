@@ -20,6 +20,16 @@
 
 #define FZ_MAGIC 0x475a4646u /* "FFZG" */
 
+/* fault injection for the failure-path tests (aoclfftz_gpu_inject_fault):
+ * process-wide, read by setup and execute */
+extern int64_t fz_inj_tma_short;   /* extra bytes each TMA tile waits for */
+extern int64_t fz_inj_ragged_wait; /* ragged dependency-wait limit (spins), 0 = default */
+extern int64_t fz_inj_ragged_dep;  /* raise the first dependent item's count at ragged setup */
+extern int64_t fz_inj_alloc_fail;  /* fail this many of the next device allocations */
+
+/* cudaMalloc, or a failure while an injected allocation failure is pending */
+int fz_dev_malloc(void **p, size_t bytes);
+
 /* logical buffers: the caller's in / out, then plan-owned scratch arrays,
  * one per use (four-step intermediates, Bluestein work arrays, the
  * half-complex work array of an out-of-place multi-dimensional c2r, dense
@@ -64,6 +74,7 @@ typedef struct fz_ragged
     int grid, smem;
     void *cap_stream;             /* stream used to capture the graph */
     void *graph, *graph_exec;     /* cudaGraph_t / cudaGraphExec_t */
+    int64_t g_spin;               /* dependency-wait limit the graph was captured with */
     const void *g_in;             /* buffers the graph was captured with */
     void *g_out;
     char summary[224];

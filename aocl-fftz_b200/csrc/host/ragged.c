@@ -379,11 +379,11 @@ FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFT
     qsort(B.items, (size_t)B.nitem, sizeof(fz_item_sort), item_cmp);
     /* device state: tables, offset lists, pass table, item table, counters, scratch */
     if (pl->blob.len &&
-        (cudaMalloc(&pl->dtab, pl->blob.len) != cudaSuccess ||
+        (fz_dev_malloc(&pl->dtab, pl->blob.len) ||
          cudaMemcpy(pl->dtab, pl->blob.p, pl->blob.len, cudaMemcpyHostToDevice) != cudaSuccess))
         goto fail_cuda;
     if (B.nind &&
-        (cudaMalloc(&rg->d_ind, sizeof(int64_t) * (size_t)B.nind) != cudaSuccess ||
+        (fz_dev_malloc(&rg->d_ind, sizeof(int64_t) * (size_t)B.nind) ||
          cudaMemcpy(rg->d_ind, B.ind, sizeof(int64_t) * (size_t)B.nind, cudaMemcpyHostToDevice) != cudaSuccess))
         goto fail_cuda;
     int64_t smem = 0;
@@ -401,17 +401,24 @@ FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFT
     flat = (fftz_ritem_t *)malloc(sizeof(fftz_ritem_t) * (size_t)B.nitem);
     if (!flat) goto fail_mem;
     for (int64_t i = 0; i < B.nitem; i++) flat[i] = B.items[i].it;
-    int ok = cudaMalloc(&rg->d_passes, sizeof(fftz_pass_t) * (size_t)B.npass) == cudaSuccess &&
+    if (fz_inj_ragged_dep > 0) /* injected: the first dependency cannot complete */
+        for (int64_t i = 0; i < B.nitem; i++)
+            if (flat[i].dep >= 0)
+            {
+                flat[i].dep_count += fz_inj_ragged_dep;
+                break;
+            }
+    int ok = !fz_dev_malloc(&rg->d_passes, sizeof(fftz_pass_t) * (size_t)B.npass) &&
              cudaMemcpy(rg->d_passes, B.passes, sizeof(fftz_pass_t) * (size_t)B.npass, cudaMemcpyHostToDevice) ==
                  cudaSuccess &&
-             cudaMalloc(&rg->d_items, sizeof(fftz_ritem_t) * (size_t)B.nitem) == cudaSuccess &&
+             !fz_dev_malloc(&rg->d_items, sizeof(fftz_ritem_t) * (size_t)B.nitem) &&
              cudaMemcpy(rg->d_items, flat, sizeof(fftz_ritem_t) * (size_t)B.nitem, cudaMemcpyHostToDevice) ==
                  cudaSuccess &&
-             cudaMalloc(&rg->d_done, sizeof(int) * (size_t)B.npass) == cudaSuccess &&
-             cudaMalloc(&rg->d_queue, sizeof(unsigned long long)) == cudaSuccess &&
-             cudaMalloc(&rg->d_err, sizeof(int)) == cudaSuccess &&
+             !fz_dev_malloc(&rg->d_done, sizeof(int) * (size_t)B.npass) &&
+             !fz_dev_malloc(&rg->d_queue, sizeof(unsigned long long)) &&
+             !fz_dev_malloc(&rg->d_err, sizeof(int)) &&
              cudaMemset(rg->d_err, 0, sizeof(int)) == cudaSuccess &&
-             (B.scratch_total == 0 || cudaMalloc(&pl->scratch, (size_t)B.scratch_total) == cudaSuccess) &&
+             (B.scratch_total == 0 || !fz_dev_malloc(&pl->scratch, (size_t)B.scratch_total)) &&
              cudaStreamCreateWithFlags((cudaStream_t *)&rg->cap_stream, cudaStreamNonBlocking) == cudaSuccess;
     if (!ok) goto fail_cuda;
     pl->scratch_bytes = B.scratch_total;
@@ -477,7 +484,9 @@ static int ragged_capture(fz_plan *pl, const void *in, void *out)
     r.in = in;
     r.out = out;
     r.scratch = pl->scratch;
-    r.spin_limit = 1LL << 26; /* about 10 s of polling at the executor's sleep */
+    /* about 10 s of polling at the executor's sleep, unless a test set a limit */
+    const int64_t spin = fz_inj_ragged_wait > 0 ? fz_inj_ragged_wait : 1LL << 26;
+    r.spin_limit = spin;
     r.dtype = pl->dtype;
     r.smem_bytes = rg->smem;
     if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -1;
@@ -503,6 +512,7 @@ static int ragged_capture(fz_plan *pl, const void *in, void *out)
     rg->graph_exec = ge;
     rg->g_in = in;
     rg->g_out = out;
+    rg->g_spin = spin;
     return 0;
 }
 
@@ -520,7 +530,8 @@ aoclfftz_error_type aoclfftz_gpu_ragged_execute(FFTZ_VOID *handle, FFTZ_VOID *in
         fz_set_error("ragged execute takes device buffers");
         return AOCLFFTZ_INVALID_INPUT;
     }
-    if (!rg->graph_exec || rg->g_in != in || rg->g_out != out)
+    const int64_t spin = fz_inj_ragged_wait > 0 ? fz_inj_ragged_wait : 1LL << 26;
+    if (!rg->graph_exec || rg->g_in != in || rg->g_out != out || rg->g_spin != spin)
         if (ragged_capture(pl, in, out))
         {
             fz_set_error("ragged execute: graph capture failed");

@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(ct_lb<T>()) fft_tma_kernel(const __grid_consta
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    mbar_expect_tx(&bar, (unsigned)(N * tpc * sizeof(T2)));
+    mbar_expect_tx(&bar, (unsigned)(N * tpc * sizeof(T2) + P.test_tx_short));
     const int64_t b0 = P.bdim[0];
     const int c0 = (int)(tf0 % b0);
     const int z = (int)(tf0 / b0);
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_pipe_kernel(const __gri
     const int64_t tf0 = tile * tpc;
     const int c0 = (int)(tf0 % b0);
     const int z = (int)(tf0 / b0);
-    mbar_expect_tx(&bar, (unsigned)(H * tpc * sizeof(T2)));
+    mbar_expect_tx(&bar, (unsigned)(H * tpc * sizeof(T2) + P.test_tx_short));
     if (MODE == 1) {
       for (int k = 0; k < H / HB; k++) tma_load_3d(stg + (size_t)k * HB * tpc, &tmap, c0 * CE, k * HB, z, &bar);
     } else {
@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_rr_kernel(const __grid_
     const int64_t tf0 = tile * tpc;
     const int c0 = (int)(tf0 % b0);
     const int z = (int)(tf0 / b0);
-    mbar_expect_tx(&bar, (unsigned)(N * tpc * sizeof(T2)));
+    mbar_expect_tx(&bar, (unsigned)(N * tpc * sizeof(T2) + P.test_tx_short));
     if (MODE == 1) {
       for (int k = 0; k < N / BOXE; k++) tma_load_3d(stg + (size_t)k * BOXE * tpc, &tmap, c0, k * BOXE, z, &bar);
     } else {
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
     const int64_t tf0 = tile * 4;
     const int c0 = (int)(tf0 % b0);
     const int z = (int)(tf0 / b0);
-    mbar_expect_tx(bar, (unsigned)(N * 4 * sizeof(T2)));
+    mbar_expect_tx(bar, (unsigned)(N * 4 * sizeof(T2) + P.test_tx_short));
 #pragma unroll 1
     for (int s = 0; s < 16; s++) {
       if (MODE == 1)

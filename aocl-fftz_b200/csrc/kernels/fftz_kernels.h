@@ -109,7 +109,8 @@ typedef struct fftz_pass
     int32_t ind_dim;
     int32_t use_tma;                    /* fetch the tile with TMA copies when the pass qualifies */
     int32_t smem_tw;                    /* compile-time kernels: copy the stage twiddles to shared memory */
-    int32_t pad2_;
+    int32_t test_tx_short;              /* fault injection (tests): TMA tiles expect this many bytes more
+                                           than their copies deliver, so the bounded tile wait runs out */
     const int64_t *ind_in, *ind_out;
 } fftz_pass_t;
 

@@ -116,7 +116,13 @@ def bind_gpu(lib):
     lib.aoclfftz_gpu_mlp_adam.restype = C.c_int32
     lib.aoclfftz_gpu_last_error.argtypes = []
     lib.aoclfftz_gpu_last_error.restype = C.c_char_p
+    lib.aoclfftz_gpu_inject_fault.argtypes = [C.c_int32, C.c_int64]
+    lib.aoclfftz_gpu_inject_fault.restype = C.c_int32
     return lib
+
+
+# fault-injection kinds of aoclfftz_gpu_inject_fault (include/aoclfftz_gpu.h)
+FAULT_NONE, FAULT_TMA_SHORT, FAULT_RAGGED_WAIT, FAULT_RAGGED_DEP, FAULT_ALLOC = 0, 1, 2, 3, 4
 
 
 def make_desc(in_ptr, out_ptr, dims, vecs, fft_type=0, direction=0, placement=1, ilp64=False, logger_mode=0,

@@ -30,6 +30,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -80,6 +81,8 @@ def parse():
     ap.add_argument("--twiddles", type=int, default=0, help="planner hint: 1 global, 2 shared-memory stage twiddles")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--selector-db", default="", help="where --workload selector writes its timing database "
+                                                      "(default: the system temporary directory)")
     return ap.parse_args()
 
 
@@ -87,6 +90,8 @@ def parse():
 # default kernels, from one ncu capture of one 2^24-point transform
 # (profiles/fourstep24_rr_passes_ncu.txt: pass A 221.2 MB, pass B 220.5 MB),
 # scaled to a launch over `batch` transforms (the traffic grows with them).
+L2_BYTES = 126 * 1000 * 1000  # B200 L2
+
 TRAFFIC_PER_TRANSFORM = {("fourstep24", 0): 221.2e6, ("fourstep24", 1): 220.5e6}
 
 
@@ -127,18 +132,42 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons sampled during a region: NVML every 2 ms
+    (the device found by its PCI bus id), else nvidia-smi every 100 ms.
+    Reading only; no GPU setting is changed."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
+        self.nv = None
         self.lines = []
+        self.samples = []
+        self.run = False
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.gpu)
+        bus = "%08X:%02X:%02X.0" % (getattr(pr, "pci_domain_id", 0), pr.pci_bus_id, pr.pci_device_id)
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
 
     def start(self):
+        try:
+            self.nv, self.h = self._nvml_handle()
+            self.smax = float(self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            self.run = True
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "100"],
@@ -148,11 +177,29 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nv, self.h
+        get_r = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while self.run:
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(get_r(h))))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nv is not None:
+            self.run = False
+            self.t.join(timeout=2)
+            sm = sorted(c for c, _ in self.samples)
+            reasons = sorted({nm for _, r in self.samples for nm, b in self.BITS.items() if r & b})
+            return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": self.smax, "reasons": reasons,
+                    "samples": len(sm), "sm_mhz_min": sm[0] if sm else None, "source": "NVML, 2 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -177,7 +224,8 @@ class ClockSampler:
                     reasons.add(nm)
         sm.sort()
         med = sm[len(sm) // 2] if sm else None
-        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi, 100 ms"}
 
 
 def load_peaks():
@@ -228,9 +276,16 @@ def run_ours(args, wl):
     x = synthetic.complex_uniform(1234 + rank, total, np.complex64 if dtype == "f32" else np.complex128)
     real = x.view(np.float32 if dtype == "f32" else np.float64)
     hx = torch.from_numpy(real).pin_memory()
-    dx = hx.to("cuda")
-    dy = torch.empty_like(dx)
-    dz = torch.empty_like(dx)
+    # inputs smaller than L2 rotate through enough buffer sets (input,
+    # intermediate, output) that a set has left the 126 MB L2 before it is
+    # used again: every step reads and writes HBM
+    set_bytes = 3 * total * esz
+    nsets = 1 if set_bytes >= 3 * L2_BYTES else -(-3 * L2_BYTES // set_bytes)
+    sets = []
+    for _ in range(nsets):
+        sets.append((hx.to("cuda"), torch.empty(2 * total, dtype=hx.dtype, device="cuda"),
+                     torch.empty(2 * total, dtype=hx.dtype, device="cuda")))
+    dx, dy, dz = sets[0]
     stream = torch.cuda.Stream()
     hints = abi.Hints()
     hints.fourstep_n1, hints.tpc_col, hints.kernel_family = args.fourstep_n1, args.tpc_col, args.family
@@ -242,14 +297,30 @@ def run_ours(args, wl):
     for h in (pf, pb):
         lib.aoclfftz_gpu_set_stream(h, C.c_void_p(stream.cuda_stream))
 
+    cur = [0]
+
     def step():
-        if lib.aoclfftz_execute(pf) or lib.aoclfftz_execute(pb):
+        a, b_, c = sets[cur[0]]
+        cur[0] = (cur[0] + 1) % nsets
+        if (lib.aoclfftz_execute_io(pf, C.c_void_p(a.data_ptr()), C.c_void_p(b_.data_ptr())) or
+                lib.aoclfftz_execute_io(pb, C.c_void_p(b_.data_ptr()), C.c_void_p(c.data_ptr()))):
             raise RuntimeError(lib.aoclfftz_gpu_last_error().decode())
 
     with torch.cuda.stream(stream):
-        for _ in range(max(args.warmup, 3)):
+        for _ in range(max(args.warmup, 3, nsets)):
             step()
     torch.cuda.synchronize()
+    # untimed soak (about half a second of steps) with its own clock record
+    soak = ClockSampler(local)
+    soak.start()
+    t_soak = time.perf_counter()
+    with torch.cuda.stream(stream):
+        while time.perf_counter() - t_soak < 0.5:
+            for _ in range(8):
+                step()
+            torch.cuda.synchronize()
+    clk_soak = soak.stop()
+    cur[0] = 0
     # correctness of the round trip on this run's data: z = N x
     zc = dz.view(torch.complex64 if dtype == "f32" else torch.complex128)
     xc = dx.view(zc.dtype)
@@ -284,6 +355,10 @@ def run_ours(args, wl):
     ms_total = max_over_ranks(ms_total, ws)
     ms = ms_total / K
     value, hbm_gbs = step_metrics(n, b, esz, ws, ms)
+    # forward outputs of the first and last transform (set 0) for the FP64 check
+    cdt = np.complex64 if dtype == "f32" else np.complex128
+    y0 = dy.cpu().numpy().view(cdt)
+    fwd_check = (n, dtype, x[:n].copy(), y0[:n].copy(), x[(b - 1) * n:].copy(), y0[(b - 1) * n:].copy())
 
     # dominant kernel: the pass with the largest summed time
     passes = [("fwd",) + p for p in pass_table(lib, pf)] + [("bwd",) + p for p in pass_table(lib, pb)]
@@ -293,8 +368,8 @@ def run_ours(args, wl):
     dom_bytes = (passes[dom][2] + passes[dom][3]) * esz
     peak, peak_kind = load_peaks()
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
-    res = dict(ms=ms, value=value, hbm_gbs=hbm_gbs, rt_err=rt_err, clocks=clk, launches=K * (npf + npb),
-               buffer_bytes=total * esz,
+    res = dict(ms=ms, value=value, hbm_gbs=hbm_gbs, rt_err=rt_err, clocks=clk, clocks_soak=clk_soak,
+               launches=K * (npf + npb), buffer_bytes=total * esz, nsets=nsets, fwd_check=fwd_check,
                roofline={"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "traffic": measured_traffic(args.workload, args, dom % npf if dom < npf else (dom - npf) % npb,
@@ -709,10 +784,10 @@ def run_selector(args, wl):
     fit_s = time.perf_counter() - t1
     rep = selector.regret_report(sel, [cs for _, cs in test])
     rep_train = selector.regret_report(sel, [cs for _, cs in train])
-    out_dir = os.path.join(ROOT, "gpurun_out")
-    os.makedirs(out_dir, exist_ok=True)
+    db = args.selector_db or os.path.join(tempfile.gettempdir(), "aoclfftz_selector_db.npz")
+    os.makedirs(os.path.dirname(os.path.abspath(db)), exist_ok=True)
     flat = [(i, j, cs[j][2], cs[j][3], json.dumps(cs[j][0])) for i, (_, cs) in enumerate(data) for j in range(len(cs))]
-    np.savez_compressed(os.path.join(out_dir, "selector_db.npz"),
+    np.savez_compressed(db,
                         problem=np.array([a for a, _, _, _, _ in flat]), cand=np.array([b for _, b, _, _, _ in flat]),
                         features=np.stack([f for _, _, f, _, _ in flat]), ms=np.array([m for _, _, _, m, _ in flat]),
                         hints=np.array([h for _, _, _, _, h in flat]),
@@ -838,6 +913,33 @@ def run_reference(args, wl):
     return base
 
 
+def l2_label(r):
+    nb = r.get("buffer_bytes", 0)
+    if r.get("nsets", 1) > 1:
+        return "inputs smaller than L2: %d rotating buffer sets of 3 x %.0f MB (%.0f MB cycled > 126 MB L2)" % (
+            r["nsets"], nb / 1e6, 3 * nb * r["nsets"] / 1e6)
+    return "inputs larger than L2 (no flush needed)" if nb > L2_BYTES else "inputs fit L2 (no flush)"
+
+
+def fp64_check(n, dtype, x0, y0, x1, y1):
+    """rel-L2 of the GPU's forward outputs in the timed run against the FP64
+    oracle: all N bins of the first transform (oracle.fft, itself pinned to
+    exact naive sums by the tests), and 32 seeded bins each of the first and
+    last transform against exact FP64 naive-DFT sums; with the bound
+    4 log2(N) eps of the dtype. About 15 s of host work at N = 2^24."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    e_all = float(oracle.rel_l2(y0, oracle.fft(x0)))
+    bins = np.sort(np.random.default_rng(2024).choice(n, size=min(32, n), replace=False))
+    e_bins = [float(oracle.rel_l2(y[bins], oracle.dft_bins(x, bins))) for x, y in ((x0, y0), (x1, y1))]
+    return {"rel_l2": e_all, "bound": oracle.tol(n, dtype),
+            "bins": "all %d bins of the first transform (FP64 fast FFT)" % n,
+            "exact_bins_rel_l2": e_bins, "exact_bins": "%d seeded bins of the first and last transform" % len(bins)}
+
+
 METRIC = "5N·log2N GFLOP/s + HBM GB/s vs plain GPU FFT at stated FP64 err, 1 B200"
 
 
@@ -871,8 +973,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(r["ms"], 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": wl["dtype"], "data": "synthetic (splitmix64 U[-1,1))",
             "config": {"workload": wl["desc"], "n": wl["n"], "batch_per_gpu": wl["batch"],
-                       "global_batch": wl["batch"] * ws, "l2": "inputs larger than L2 (no flush needed)"
-                       if r.get("buffer_bytes", 0) > 126e6 else "inputs fit L2 (no flush)",
+                       "global_batch": wl["batch"] * ws, "l2": l2_label(r),
                        "parallelism": "replicas dp%d" % ws},
             "hbm_gbs": round(r["hbm_gbs"], 1), "hbm_frac_of_measured": round(r["hbm_gbs"] / peak, 4),
             "gpu_launches": r["launches"], "clocks": r["clocks"], "round_trip_rel_l2": r["rt_err"]}
@@ -882,7 +983,16 @@ def main():
     line.update(r.get("extra", {}))
     if "e2e" in r:
         line["e2e"] = r["e2e"]
+    if "clocks_soak" in r:
+        line["clocks_soak"] = r["clocks_soak"]
     if ws == 1 and not args.no_cpu_baseline and not wl.get("ragged") and not wl.get("selector"):
+        # the CPU leg: the reference timed on the host cores, and the FP64
+        # oracle as the checker of this run's forward outputs
+        if r.get("fwd_check") is not None:
+            try:
+                line["fp64_oracle"] = fp64_check(*r["fwd_check"])
+            except Exception as e:
+                line["fp64_oracle"] = {"unavailable": str(e)}
         try:
             line["cpu_baseline"] = cpu_baseline(wl)
         except Exception as e:  # the baseline is reported, never required

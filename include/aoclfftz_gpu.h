@@ -113,6 +113,34 @@ FFTZ_INT32 aoclfftz_gpu_mlp_adam(float *params, const float *grads, float *m, fl
 /* Text of the last error recorded by this thread (empty if none). */
 const FFTZ_CHAR *aoclfftz_gpu_last_error(FFTZ_VOID);
 
+/* Fault injection for failure-path tests (no reference counterpart: the
+ * reference's own tests have none). Process-wide; value 0 switches a kind
+ * off, kind AOCLFFTZ_GPU_FAULT_NONE switches every kind off. Nothing here
+ * makes the GPU fault or hang: every injected failure ends in a bounded wait
+ * or a refused allocation that the host reports.
+ *   TMA_SHORT   the TMA-fed kernels' tiles wait for `value` bytes more than
+ *               their copies deliver (<= 2^20): each tile's bounded wait runs
+ *               out, execute / synchronize report AOCLFFTZ_EXECUTION_FAILURE.
+ *               A real wait that runs out may leave copies in flight that land
+ *               later: that pass's results and those of later work on the
+ *               same stream are invalid.
+ *   RAGGED_WAIT dependency waits of ragged executors captured from now on
+ *               give up after `value` polls (about 100 ns each).
+ *   RAGGED_DEP  ragged plans set up from now on wait for `value` more tiles
+ *               than the first dependency has (that wait cannot complete).
+ *   ALLOC       the next `value` device allocations of setup / execute fail
+ *               (setup returns NULL, execute AOCLFFTZ_MEMORY_FAILURE).
+ * Returns 0, or -1 for an unknown kind or value. */
+enum
+{
+    AOCLFFTZ_GPU_FAULT_NONE = 0,
+    AOCLFFTZ_GPU_FAULT_TMA_SHORT = 1,
+    AOCLFFTZ_GPU_FAULT_RAGGED_WAIT = 2,
+    AOCLFFTZ_GPU_FAULT_RAGGED_DEP = 3,
+    AOCLFFTZ_GPU_FAULT_ALLOC = 4
+};
+FFTZ_INT32 aoclfftz_gpu_inject_fault(FFTZ_INT32 kind, FFTZ_INT64 value);
+
 /* No-allocation execute. No counterpart in the reference, which never needs
  * device memory. For callers that may not allocate device memory when they
  * transform: another allocator owns the device's memory, or a latency-critical

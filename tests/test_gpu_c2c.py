@@ -145,10 +145,21 @@ def test_size_one_and_empty_batch():
 
 
 def test_config1_shape():
-    """4096-point fp32 transforms, batch 1024, out of place, forward then backward."""
+    """The plain c2c workload's shape: 4096-point fp32 transforms, batch 1024,
+    out of place, forward then backward, against the FP64 oracle and the
+    reference library run on the same seeded inputs."""
     n, b = 4096, 1024
-    check_c2c("f32", [(n, 1, 1)], [(b, n, n)], 0, compare_ref=False)
-    check_c2c("f32", [(n, 1, 1)], [(b, n, n)], 1, compare_ref=False)
+    check_c2c("f32", [(n, 1, 1)], [(b, n, n)], 0)
+    check_c2c("f32", [(n, 1, 1)], [(b, n, n)], 1)
+
+
+def test_config2_transform_against_reference():
+    """One transform of the four-step workload: fp32 N = 2^24 (4096 x 4096),
+    out of place, both directions, against the FP64 oracle and the reference
+    library's own four-step run on the same seeded input."""
+    n = 1 << 24
+    check_c2c("f32", [(n, 1, 1)], [(1, n, n)], 0)
+    check_c2c("f32", [(n, 1, 1)], [(1, n, n)], 1, seed=2)
 
 
 def test_bit_reproducible():

@@ -56,7 +56,7 @@ def check_real(dtype, shape, batch=1, inplace=False, seed=3, compare_ref=True):
         r_raw = oracle.ref_execute(dtype, dims, vecs, raw, out_sc, 1, 0, pl)
         R = gather(r_raw, [(d[0], d[2]) for d in dims], [(batch, ctot)], dtype, n0=h0)
         # the reference's own error vs the exact DFT widens the bound where it exceeds the
-        # dtype bound (f64 odd length 15: 8e-13, see the known divergences in DESIGN.md)
+        # dtype bound (the reference's f64 r2c of odd length 15 is off by 8e-13 relative)
         assert oracle.rel_l2(X, R) <= 2 * tol + oracle.rel_l2(R, ref)
     # backward c2r of the oracle spectrum
     cdims = [(rdims[i], c_str[i], r_str[i]) for i in range(len(rdims))]

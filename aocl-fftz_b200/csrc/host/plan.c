@@ -335,6 +335,30 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         finish_launch_shape(pl, k, nslots, maxthr);
     }
     if (k->smem_tw && fftz_pass_smem_bytes(k) > fftz_smem_limit()) k->smem_tw = 0;
+    /* runtime-radix lines: the ping-pong kernel (two shared-memory buffers,
+     * one butterfly per thread at a time, 256 threads) when both buffers fit;
+     * kernel_family 12 keeps the in-place kernel */
+    if (k->variant == FFTZ_VAR_GENERIC && !ragged_mode(pl) && pl->hints.kernel_family != 12)
+    {
+        const int esz = pl->dtype == 0 ? 8 : 16;
+        const int32_t sst = fftz_smem_stride(pl->dtype, nslots);
+        const int colm = (k->in_mode == 1 || k->out_mode == 1);
+        int64_t want = (pl->dtype == 0 ? 2048 : 1024) / n;
+        if (colm && want < (pl->dtype == 0 ? 8 : 4)) want = pl->dtype == 0 ? 8 : 4;
+        if (colm && pl->hints.tpc_col > 0) want = pl->hints.tpc_col;
+        if (!colm && pl->hints.tpc_row > 0) want = pl->hints.tpc_row;
+        if (want < 1) want = 1;
+        if (want > 64) want = 64;
+        if (want > k->ntf) want = k->ntf;
+        while (want > 1 && 2 * want * sst * esz + 24 * want + 8 * FFTZ_MAX_STAGES > fftz_smem_limit()) want--;
+        if (2 * want * (int64_t)sst * esz + 24 * want + 8 * FFTZ_MAX_STAGES <= fftz_smem_limit())
+        {
+            k->variant = FFTZ_VAR_GENERIC_PP;
+            k->tpc = (int32_t)want;
+            k->sstride = sst;
+            k->tpt = (int32_t)(256 / want > 0 ? 256 / want : 1);
+        }
+    }
     if (fftz_pass_smem_bytes(k) > fftz_smem_limit())
     {
         fz_set_error("length %lld does not fit shared memory", (long long)n);
@@ -360,7 +384,9 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         if (p->off_tw < 0) return NULL;
     }
     snprintf(p->what, sizeof(p->what), "%s n=%lld x%lld",
-             k->variant == FFTZ_VAR_GENERIC ? "generic" : (is_pipe_variant(k->variant) ? "pipe" : "fast"),
+             k->variant == FFTZ_VAR_GENERIC ? "generic"
+             : k->variant == FFTZ_VAR_GENERIC_PP ? "generic-pp"
+                                                 : (is_pipe_variant(k->variant) ? "pipe" : "fast"),
              (long long)n, (long long)k->ntf);
     return p;
 }

@@ -105,6 +105,8 @@ int32_t fftz_fast_tw_entries(int n) {
 int64_t fftz_pass_smem_bytes(const fftz_pass_t *p) {
   if (p->variant == FFTZ_VAR_TC) return fftz_tc_smem_bytes();
   const int64_t esz = p->dtype == 0 ? 8 : 16;
+  if (p->variant == FFTZ_VAR_GENERIC_PP)
+    return 2 * (int64_t)p->tpc * p->sstride * esz + 3 * 8 * (int64_t)p->tpc + 8 * FFTZ_MAX_STAGES;
   if (is_pipe(p)) return 2 * (int64_t)p->tpc * p->sstride * esz + 9 * 8 * (int64_t)p->tpc;
   int64_t b = (int64_t)p->tpc * p->sstride * esz + 3 * 8 * (int64_t)p->tpc;
   if (p->smem_tw) b += 16 + (int64_t)fftz_fast_tw_entries(p->n) * esz;  // shared copy of the stage twiddles
@@ -130,6 +132,8 @@ int fftz_launch_pass(const fftz_pass_t *p, void *stream) {
   if (p->variant == FFTZ_VAR_GENERIC) {
     fn = p->dtype == 0 ? (const void *)&fftz::fft_smem_kernel_occ3<float>
                        : (const void *)&fftz::fft_smem_kernel<double>;
+  } else if (p->variant == FFTZ_VAR_GENERIC_PP) {
+    fn = p->dtype == 0 ? (const void *)&fftz::fft_pp_kernel<float> : (const void *)&fftz::fft_pp_kernel<double>;
   } else {
     fn = fast_kernel(p->dtype, fftz::ct_log2(p->n), p->variant);
   }
@@ -142,7 +146,7 @@ int fftz_launch_pass(const fftz_pass_t *p, void *stream) {
     if (e != cudaSuccess) return (int)e;
     if (nopted[dev] < 96) opted[dev][nopted[dev]++] = fn;
   }
-  const dim3 block((unsigned)(p->tpc * p->tpt));
+  const dim3 block(p->variant == FFTZ_VAR_GENERIC_PP ? 256u : (unsigned)(p->tpc * p->tpt));
   const size_t smem = (size_t)fftz_pass_smem_bytes(p);
   dim3 grid((unsigned)nblk);
   if (is_pipe(p)) {

@@ -346,6 +346,187 @@ __device__ __forceinline__ void generic_tile(const fftz_pass_t &P, int64_t blk, 
   if (!P.fuse_store) store_phase<T>(P, sdata, s_out, s_col);
 }
 
+// ------------------------------------------------------------ ping-pong tile
+//
+// Runtime-radix stages over two shared-memory buffers per transform (stage s
+// reads one, writes the other): every stage is a loop in which a thread takes
+// one radix-R butterfly at a time, so only R values are live, and the
+// butterflies of all the CTA's transforms are spread over all its threads
+// (item i -> transform p and butterfly bf by multiply-high division with
+// per-stage reciprocals, no runtime / or %). One barrier per stage. Used when
+// both buffers fit shared memory; longer lines keep the in-place tile above.
+
+// m = ceil(2^32 / d) for d > 1 (0 for d = 1): x / d = umulhi(x, m) exactly
+// while x * d < 2^32, which holds for every index here (x * d < 2^31)
+__host__ __device__ __forceinline__ uint32_t pp_magic(uint32_t d) {
+  return d <= 1 ? 0u : (uint32_t)((0xFFFFFFFFull + d) / d);
+}
+__device__ __forceinline__ int pp_div(int x, uint32_t m) { return m ? (int)__umulhi((uint32_t)x, m) : x; }
+
+// One stage of radix R. MAP (first / last fused stage): 0 lanes along
+// elements (rows), 1 lanes along transforms (columns).
+template <typename T, int R, bool FROMG, bool TOG, int MAP>
+__device__ __forceinline__ void pp_stage(const fftz_pass_t &P, const typename Cplx<T>::type *src,
+                                         typename Cplx<T>::type *dst, int s, int Ns, uint32_t mNs, int nbf,
+                                         uint32_t mnbf, uint32_t mtpc, const int64_t *s_in, const int64_t *s_out,
+                                         const int64_t *s_col) {
+  typedef typename Cplx<T>::type T2;
+  constexpr int SH = Cplx<T>::PADSH;
+  const int tpc = P.tpc, sst = P.sstride;
+  const int total = tpc * nbf;
+  const T2 *tw = (const T2 *)P.tw + P.tw_off[s];
+  const bool cjin = FROMG && (P.flags & FFTZ_F_CONJ_IN) != 0;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    int p, bf;
+    if (MAP == 1) {
+      bf = pp_div(i, mtpc);
+      p = i - bf * tpc;
+    } else {
+      p = pp_div(i, mnbf);
+      bf = i - p * nbf;
+    }
+    T2 v[R];
+    if (FROMG) {
+      const int64_t col = s_col[p];
+      const T2 *gin = (const T2 *)P.in + s_in[p];
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        T2 x = zero2<T2>();
+        if (col >= 0) x = gin[(int64_t)(bf + r * nbf) * P.ies];
+        if (cjin) x.y = -x.y;
+        v[r] = x;
+      }
+    } else {
+      const T2 *sp = src + (size_t)p * sst;
+#pragma unroll
+      for (int r = 0; r < R; r++) v[r] = sp[phys<SH>(bf + r * nbf)];
+    }
+    const int g = pp_div(bf, mNs);
+    const int k = bf - g * Ns;
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; r++) v[r] = cmul(v[r], __ldg(tw + (r - 1) * Ns + k));
+    }
+    Dft<R>::template apply<T, T2>(v);
+    const int d0 = g * Ns * R + k;
+    if (TOG) {
+      const int64_t col = s_col[p];
+      if (col >= 0) {
+#pragma unroll
+        for (int r = 0; r < R; r++) store_complex<T>(P, v[r], d0 + r * Ns, col, s_out[p]);
+      }
+    } else {
+      T2 *dp = dst + (size_t)p * sst;
+#pragma unroll
+      for (int r = 0; r < R; r++) dp[phys<SH>(d0 + r * Ns)] = v[r];
+    }
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void pp_stage_role(const fftz_pass_t &P, const typename Cplx<T>::type *src,
+                                              typename Cplx<T>::type *dst, int s, int Ns, uint32_t mNs, int nbf,
+                                              uint32_t mnbf, uint32_t mtpc, bool from_g, bool to_g,
+                                              const int64_t *s_in, const int64_t *s_out, const int64_t *s_col) {
+  if (from_g && to_g) {
+    if (P.in_mode == 1)
+      pp_stage<T, R, true, true, 1>(P, src, dst, s, Ns, mNs, nbf, mnbf, mtpc, s_in, s_out, s_col);
+    else
+      pp_stage<T, R, true, true, 0>(P, src, dst, s, Ns, mNs, nbf, mnbf, mtpc, s_in, s_out, s_col);
+  } else if (from_g) {
+    if (P.in_mode == 1)
+      pp_stage<T, R, true, false, 1>(P, src, dst, s, Ns, mNs, nbf, mnbf, mtpc, s_in, s_out, s_col);
+    else
+      pp_stage<T, R, true, false, 0>(P, src, dst, s, Ns, mNs, nbf, mnbf, mtpc, s_in, s_out, s_col);
+  } else if (to_g) {
+    if (P.out_mode == 1)
+      pp_stage<T, R, false, true, 1>(P, src, dst, s, Ns, mNs, nbf, mnbf, mtpc, s_in, s_out, s_col);
+    else
+      pp_stage<T, R, false, true, 0>(P, src, dst, s, Ns, mNs, nbf, mnbf, mtpc, s_in, s_out, s_col);
+  } else {
+    pp_stage<T, R, false, false, 0>(P, src, dst, s, Ns, mNs, nbf, mnbf, mtpc, s_in, s_out, s_col);
+  }
+}
+
+// Shared memory of a ping-pong tile: two buffers of tpc * sstride complex,
+// then in / out offsets and columns, then two reciprocals per stage.
+template <typename T>
+__device__ __forceinline__ void generic_tile_pp(const fftz_pass_t &P, int64_t blk, unsigned char *smem_raw) {
+  typedef typename Cplx<T>::type T2;
+  constexpr int SH = Cplx<T>::PADSH;
+  T2 *buf0 = (T2 *)smem_raw;
+  T2 *buf1 = buf0 + (size_t)P.tpc * P.sstride;
+  int64_t *s_in = (int64_t *)(buf1 + (size_t)P.tpc * P.sstride);
+  int64_t *s_out = s_in + P.tpc;
+  int64_t *s_col = s_out + P.tpc;
+  uint32_t *s_mag = (uint32_t *)(s_col + P.tpc);  // [s]: Ns, n / R
+  const int64_t tf0 = blk * P.tpc;
+  for (int p = threadIdx.x; p < P.tpc; p += blockDim.x) batch_offsets(P, tf0 + p, s_in + p, s_out + p, s_col + p);
+  if (threadIdx.x < P.nstages) {
+    int Ns = 1;
+    for (int s = 0; s < (int)threadIdx.x; s++) Ns *= P.radix[s];
+    s_mag[2 * threadIdx.x] = pp_magic((uint32_t)Ns);
+    s_mag[2 * threadIdx.x + 1] = pp_magic((uint32_t)(P.n / P.radix[threadIdx.x]));
+  }
+  __syncthreads();
+  const uint32_t mtpc = pp_magic((uint32_t)P.tpc);
+  const int nsweeps = (P.flags & FFTZ_F_MID_TAB) ? 2 : 1;
+  T2 *cur = buf0, *nxt = buf1;
+  if (!P.fuse_load) load_phase<T>(P, cur, s_in, s_col);
+  for (int sw = 0; sw < nsweeps; sw++) {
+    int Ns = 1;
+    for (int s = 0; s < P.nstages; s++) {
+      const bool from_g = P.fuse_load && sw == 0 && s == 0;
+      const bool to_g = P.fuse_store && sw == nsweeps - 1 && s == P.nstages - 1;
+      const int R = P.radix[s];
+      const int nbf = P.n / R;
+      const uint32_t mNs = s_mag[2 * s], mnbf = s_mag[2 * s + 1];
+      switch (R) {
+        case 2: pp_stage_role<T, 2>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+        case 3: pp_stage_role<T, 3>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+        case 4: pp_stage_role<T, 4>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+        case 5: pp_stage_role<T, 5>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+        case 7: pp_stage_role<T, 7>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+        case 8: pp_stage_role<T, 8>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+        case 11: pp_stage_role<T, 11>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+        case 13: pp_stage_role<T, 13>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+        default: pp_stage_role<T, 16>(P, cur, nxt, s, Ns, mNs, nbf, mnbf, mtpc, from_g, to_g, s_in, s_out, s_col); break;
+      }
+      if (!to_g) {
+        __syncthreads();
+        T2 *t = cur;
+        cur = nxt;
+        nxt = t;
+      }
+      Ns *= R;
+    }
+    if (sw == 0 && nsweeps == 2) {
+      // between the sweeps: v = conj(v) * mid_tab[e] (spectrum product of Bluestein)
+      const T2 *mt = (const T2 *)P.mid_tab;
+      for (int i = threadIdx.x; i < P.tpc * P.n; i += blockDim.x) {
+        const int p = i / P.n;
+        const int e = i - p * P.n;
+        const int64_t c = s_col[p];
+        if (c < 0) continue;
+        T2 *a = cur + (size_t)p * P.sstride + phys<SH>(e);
+        T2 v = *a;
+        v.y = -v.y;
+        *a = cmul(v, __ldg(mt + e + c * P.mid_cs));
+      }
+      __syncthreads();
+    }
+  }
+  if (!P.fuse_store) store_phase<T>(P, cur, s_out, s_col);
+}
+
+// 256 threads; float 80 registers (3 CTAs per SM), double 128 (2 CTAs): the
+// bounds at which the inlined radix paths keep their spills to a few bytes
+template <typename T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) fft_pp_kernel(const __grid_constant__ fftz_pass_t P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  generic_tile_pp<T>(P, (int64_t)blockIdx.x, smem_raw);
+}
+
 // float: at most 80 registers (3 CTAs of 256 threads per SM) -- measured on
 // B200 1.6-2.8x faster than the unbounded build for mixed-radix lines
 // (n = 1000 ... 44100); double keeps the plain thread bound (a minimum-blocks

@@ -53,6 +53,7 @@ enum fftz_out_kind {
 #define FFTZ_VAR_PIPE_TW4 7  /* as PIPE with the four-step twiddle epilogue         */
 #define FFTZ_VAR_TC 8        /* 4096-point rows as two radix-64 tensor-core GEMM stages */
 #define FFTZ_VAR_FAST_REAL 9 /* packed real line: generic load/store phases, compile-time stages */
+#define FFTZ_VAR_GENERIC_PP 10 /* runtime radix list over two shared-memory buffers, 256 threads */
 
 /* pass flags */
 #define FFTZ_F_CONJ_IN    0x01 /* conjugate each loaded value (after kind decode) */

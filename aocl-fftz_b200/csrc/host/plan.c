@@ -357,6 +357,12 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
             k->tpc = (int32_t)want;
             k->sstride = sst;
             k->tpt = (int32_t)(256 / want > 0 ? 256 / want : 1);
+            /* complex lines read HBM in their first stage and write it in
+             * their last (the load / store phases stay for the other kinds
+             * and for load-side tables) */
+            k->fuse_load = k->nstages > 0 && k->in_kind == FFTZ_IN_COMPLEX && k->nload == n &&
+                           !(flags & FFTZ_F_PRE_TAB);
+            k->fuse_store = k->nstages > 0 && k->out_kind == FFTZ_OUT_COMPLEX && k->nstore == n;
         }
     }
     if (fftz_pass_smem_bytes(k) > fftz_smem_limit())

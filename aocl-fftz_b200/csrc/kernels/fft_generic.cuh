@@ -376,6 +376,10 @@ __device__ __forceinline__ void pp_stage(const fftz_pass_t &P, const typename Cp
   const int total = tpc * nbf;
   const T2 *tw = (const T2 *)P.tw + P.tw_off[s];
   const bool cjin = FROMG && (P.flags & FFTZ_F_CONJ_IN) != 0;
+  // stores with at most a conjugation take the direct path
+  const bool plain_out =
+      TOG && (P.flags & (FFTZ_F_TW4 | FFTZ_F_POST_TAB | FFTZ_F_SCALE)) == 0 && P.post_n == 0;
+  const bool cjout = TOG && (P.flags & FFTZ_F_CONJ_OUT) != 0;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     int p, bf;
     if (MAP == 1) {
@@ -412,8 +416,19 @@ __device__ __forceinline__ void pp_stage(const fftz_pass_t &P, const typename Cp
     if (TOG) {
       const int64_t col = s_col[p];
       if (col >= 0) {
+        if (plain_out) {
+          T2 *gout = (T2 *)P.out + s_out[p];
+          const int64_t oes = P.oes;
 #pragma unroll
-        for (int r = 0; r < R; r++) store_complex<T>(P, v[r], d0 + r * Ns, col, s_out[p]);
+          for (int r = 0; r < R; r++) {
+            T2 y = v[r];
+            if (cjout) y.y = -y.y;
+            gout[(int64_t)(d0 + r * Ns) * oes] = y;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; r++) store_complex<T>(P, v[r], d0 + r * Ns, col, s_out[p]);
+        }
       }
     } else {
       T2 *dp = dst + (size_t)p * sst;

@@ -851,12 +851,79 @@ def time_reference(wl, threads, transforms, steps, warmup, min_time=None):
     return el / k, k, err
 
 
+def time_reference_ragged(wl, threads, steps, warmup, min_time=None, sample=None):
+    """The reference library on the ragged batch: one reference plan per
+    transform (setup not timed), all forward then all backward executes back
+    to back -- the reference has no ragged API. `sample` bounds the run to the
+    first transforms of the same seeded batch (the setup of the long-prime
+    plans alone takes seconds each). Returns (seconds per step, steps timed,
+    worst round-trip error, flops per step)."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from aoclfftz_b200 import abi, synthetic
+
+    L = oracle.ref_lib()
+    dtype = wl["dtype"]
+    cd = np.complex64 if dtype == "f32" else np.complex128
+    sizes = synthetic.ragged_sizes(4242, wl["batch"], 2, 65536)[:sample]
+    total = int(sum(sizes))
+    x = synthetic.complex_normal(4243, total, cd)
+    y = np.empty_like(x)
+    z = np.empty_like(x)
+    offs = np.cumsum([0] + sizes[:-1])
+    esz = x.itemsize
+    plans, keep = [], []
+    for a, b_, d in ((x, y, 0), (y, z, 1)):
+        for o, n in zip(offs, sizes):
+            desc, k = abi.make_desc(a.ctypes.data + int(o) * esz, b_.ctypes.data + int(o) * esz, [(n, 1, 1)],
+                                    [(1, n, n)], 0, d, 1, num_threads=threads, opt_level=3)
+            h = abi.setup(L, desc, dtype)
+            if not h:
+                raise RuntimeError("reference setup failed for n=%d" % n)
+            plans.append(h)
+            keep.append(k)
+
+    def step():
+        for h in plans:
+            if L.aoclfftz_execute(h) != 0:
+                raise RuntimeError("reference execute failed")
+
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        step()
+        k += 1
+        el = time.perf_counter() - t0
+        if steps is not None and k >= steps:
+            break
+        if steps is None and el >= min_time:
+            break
+    for h in plans:
+        L.aoclfftz_destroy(h)
+    err = max(float(np.linalg.norm(z[o:o + n] / n - x[o:o + n]) / max(np.linalg.norm(x[o:o + n]), 1e-30))
+              for o, n in zip(offs, sizes))
+    flops = 2 * sum(5.0 * n * math.log2(n) for n in sizes if n > 1)
+    return el / k, k, err, flops
+
+
 def flops_per_transform(n):
     return 2 * 5.0 * n * math.log2(n)  # forward + backward
 
 
 def cpu_baseline(wl):
     threads = os.cpu_count() or 1
+    if wl.get("ragged"):
+        sec, k, err, flops = time_reference_ragged(wl, threads, None, 1, min_time=10.0, sample=512)
+        sec1, k1, _, flops1 = time_reference_ragged(wl, 1, None, 0, min_time=5.0, sample=128)
+        return {"value": round(flops / sec / 1e9, 3), "unit": "GFLOP/s", "cores": threads, "kind": "reference",
+                "sample": "the first 512 of the %d seeded transforms, fwd+bwd per rep as 1024 reference plans "
+                          "(one per transform and direction), %d reps (%.1f s), OpenMP %d threads, opt_level 3; "
+                          "value_1_thread: the first 128, one thread" % (wl["batch"], k, sec * k, threads),
+                "value_1_thread": round(flops1 / sec1 / 1e9, 3), "round_trip_rel_l2": err}
     if wl.get("real3d"):
         sec, k, err = time_reference_real3d(wl, threads, None, 0, min_time=10.0)
         return {"value": round(real3d_metrics(wl["real3d"], sec * 1e3)[0], 3), "unit": "GFLOP/s",
@@ -885,6 +952,21 @@ def run_reference(args, wl):
     threads = os.cpu_count() or 1
     n = wl["n"]
     t = wl["batch"]
+    if wl.get("selector"):
+        return {"impl": "reference", "unavailable": "the reference has no plan selector to time"}
+    if wl.get("ragged"):
+        sec, k, err, flops = time_reference_ragged(wl, threads, args.steps, args.warmup, sample=1024)
+        v = flops / sec / 1e9
+        return {"metric": METRIC, "value": round(v, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"], "data": "synthetic (splitmix64 N(0,1))",
+                "impl": "reference", "config": {"workload": wl["desc"], "batch": wl["batch"]},
+                "cpu_baseline": {"value": round(v, 3), "unit": "GFLOP/s", "cores": threads, "kind": "reference",
+                                 "sample": "the first 1024 of the %d seeded transforms per step, one reference "
+                                           "plan per transform and direction, OpenMP %d threads"
+                                           % (wl["batch"], threads)},
+                "e2e": {"value": round(v, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "round_trip_rel_l2": err}
     if wl.get("real3d"):
         sec, k, err = time_reference_real3d(wl, threads, args.steps, args.warmup)
         v = real3d_metrics(wl["real3d"], sec * 1e3)[0]
@@ -985,7 +1067,7 @@ def main():
         line["e2e"] = r["e2e"]
     if "clocks_soak" in r:
         line["clocks_soak"] = r["clocks_soak"]
-    if ws == 1 and not args.no_cpu_baseline and not wl.get("ragged") and not wl.get("selector"):
+    if ws == 1 and not args.no_cpu_baseline and not wl.get("selector"):
         # the CPU leg: the reference timed on the host cores, and the FP64
         # oracle as the checker of this run's forward outputs
         if r.get("fwd_check") is not None:

@@ -30,6 +30,9 @@ extern int64_t fz_inj_alloc_fail;  /* fail this many of the next device allocati
 /* cudaMalloc, or a failure while an injected allocation failure is pending */
 int fz_dev_malloc(void **p, size_t bytes);
 
+/* shared memory a ragged executor tile may use (its CTAs run several per SM) */
+int64_t fz_ragged_smem_cap(int dtype);
+
 /* logical buffers: the caller's in / out, then plan-owned scratch arrays,
  * one per use (four-step intermediates, Bluestein work arrays, the
  * half-complex work array of an out-of-place multi-dimensional c2r, dense

@@ -164,6 +164,13 @@ static int set_batch(fftz_pass_t *k, const fz_dim *b, int nb, int keep_first)
     return 0;
 }
 
+/* shared memory of one ping-pong tile holding one line of n */
+static int64_t pp_one_line_bytes(int dtype, int64_t n)
+{
+    const int64_t esz = dtype == 0 ? 8 : 16;
+    return 2 * (int64_t)fftz_smem_stride(dtype, (int32_t)n) * esz + 24 + 8 * FFTZ_MAX_STAGES;
+}
+
 /* transforms per CTA: enough columns for coalesced column access, enough
  * work per CTA for short rows, bounded by threads and shared memory (two
  * slots for the double-buffered kernels) */
@@ -311,6 +318,10 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         }
         k->tpt = k->nstages ? fftz_threads_per_transform(pl->dtype, (int)n, k->nstages, k->radix) : 1;
         maxthr = fftz_generic_max_threads();
+        /* lines longer than the in-place tile's thread budget run as ping-pong
+         * tiles (chosen below) */
+        if (k->tpt > maxthr && pl->hints.kernel_family != 12 && pp_one_line_bytes(pl->dtype, n) <= fftz_smem_limit())
+            k->tpt = maxthr;
         if (k->tpt > maxthr)
         {
             fz_set_error("length %lld exceeds the generic kernel's thread budget", (long long)n);
@@ -338,7 +349,7 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
     /* runtime-radix lines: the ping-pong kernel (two shared-memory buffers,
      * one butterfly per thread at a time, 256 threads) when both buffers fit;
      * kernel_family 12 keeps the in-place kernel */
-    if (k->variant == FFTZ_VAR_GENERIC && !ragged_mode(pl) && pl->hints.kernel_family != 12)
+    if (k->variant == FFTZ_VAR_GENERIC && pl->hints.kernel_family != 12)
     {
         const int esz = pl->dtype == 0 ? 8 : 16;
         const int32_t sst = fftz_smem_stride(pl->dtype, nslots);
@@ -406,7 +417,10 @@ static int single_pass_ok(const fz_plan *pl, int64_t n)
     if (!generic_only(pl) && is_pow2(n) && n <= fast_max_n(pl)) return 1;
     int32_t r[FFTZ_MAX_STAGES];
     int s = generic_radices(n, r);
-    if (s < 0) return 0;
+    if (s < 0 || n > (1 << 20)) return 0;
+    /* the executor's tiles (ragged batches) are ping-pong tiles within its cap */
+    if (ragged_mode(pl)) return pp_one_line_bytes(pl->dtype, n) <= fz_ragged_smem_cap(pl->dtype);
+    if (pl->hints.kernel_family != 12 && pp_one_line_bytes(pl->dtype, n) <= fftz_smem_limit()) return 1;
     int tpt = fftz_threads_per_transform(pl->dtype, (int)n, s, r);
     if (tpt < 1 || tpt > fftz_generic_max_threads()) return 0;
     int64_t esz = pl->dtype == 0 ? 8 : 16;

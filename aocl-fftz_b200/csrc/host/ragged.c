@@ -76,6 +76,13 @@ static void resolve(int id, int64_t io_off_bytes, const int64_t *soff, int32_t *
 
 #define RG_THREADS 256
 
+/* The executor's shared memory per CTA is the largest of its passes', so
+ * every tile shape stays within 44 KB (float: five CTAs per SM, the
+ * executor's register bound) or 100 KB (double: two CTAs per SM). Measured on
+ * B200 (4096 float transforms): float ping-pong tiles of up to 72 KB made the
+ * whole launch 1.353 -> 1.688 ms although their own class got faster. */
+int64_t fz_ragged_smem_cap(int dtype) { return dtype == 0 ? 44 * 1024 : 100 * 1024; }
+
 /* Launch shape of one pass inside the executor (256-thread CTAs): a
  * compile-time tile with tpc * tpt == 256 where the executor has one,
  * otherwise the generic tile with as many transforms as fit (loads and stores
@@ -98,17 +105,26 @@ static int ragged_shape(fftz_pass_t *k, int dtype, int64_t smem_cap)
             return 0;
         }
     }
-    if (k->variant != FFTZ_VAR_GENERIC)
+    /* everything else runs as a ping-pong tile (the same radix list and
+     * twiddle table; tables and other element kinds through its load / store
+     * phases): as many lines as fit the cap, up to about 4096 elements */
+    if (k->variant != FFTZ_VAR_GENERIC_PP)
     {
-        k->variant = FFTZ_VAR_GENERIC;
-        k->fuse_load = 0;
-        k->fuse_store = 0;
+        k->variant = FFTZ_VAR_GENERIC_PP;
+        k->fuse_load = k->nstages > 0 && k->in_kind == FFTZ_IN_COMPLEX && k->nload == k->n &&
+                       !(k->flags & FFTZ_F_PRE_TAB);
+        k->fuse_store = k->nstages > 0 && k->out_kind == FFTZ_OUT_COMPLEX && k->nstore == k->n;
     }
-    if (k->tpt < 1 || k->tpt > RG_THREADS) return -1;
-    for (int tpc = RG_THREADS / k->tpt; tpc >= 1; tpc--)
+    int tpc = (int)((dtype == 0 ? 4096 : 2048) / k->n);
+    if (colmap && tpc < (dtype == 0 ? 8 : 4)) tpc = dtype == 0 ? 8 : 4;
+    if (tpc < 1) tpc = 1;
+    if (tpc > 64) tpc = 64;
+    if (tpc > k->ntf) tpc = (int)k->ntf;
+    for (; tpc >= 1; tpc--)
     {
         k->tpc = tpc;
-        k->sstride = colmap ? fftz_smem_stride_cols(dtype, nslots, tpc) : fftz_smem_stride(dtype, nslots);
+        k->sstride = fftz_smem_stride(dtype, nslots);
+        k->tpt = RG_THREADS / tpc > 0 ? RG_THREADS / tpc : 1;
         if (fftz_pass_smem_bytes(k) <= smem_cap) return 0;
     }
     return -1;
@@ -333,7 +349,7 @@ FFTZ_VOID *aoclfftz_gpu_ragged_setup(FFTZ_INT32 dtype, FFTZ_INT32 direction, FFT
     B.dtype = dtype;
     B.direction = direction;
     B.csz = dtype == 0 ? 8 : 16;
-    B.smem_cap = dtype == 0 ? 72 * 1024 : 100 * 1024;
+    B.smem_cap = fz_ragged_smem_cap(dtype);
     int64_t next_in = 0, next_out = 0;
     for (int64_t i = 0; i < count; i++)
     {

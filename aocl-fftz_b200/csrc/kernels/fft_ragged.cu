@@ -105,7 +105,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 2) fft_ragged_kernel
       }
     }
     __syncthreads();
-    if (s_ok && !ragged_fast<T>(sP, item.blk, smem_raw)) generic_tile<T>(sP, item.blk, smem_raw);
+    // tiles without a compile-time form are ping-pong tiles (the host plans
+    // every other pass that way)
+    if (s_ok && !ragged_fast<T>(sP, item.blk, smem_raw)) generic_tile_pp<T>(sP, item.blk, smem_raw);
     __syncthreads();
     // only passes that another pass waits for publish their tiles (the fence
     // waits for the tile's stores, which nothing else needs to do)

@@ -507,6 +507,18 @@ static int prepare_chunks(fz_plan *pl)
 }
 
 /* Launches the passes of plan `ch` with the given buffer bases on stream st. */
+/* The blocked four-step intermediate needs its column pass on the split
+ * kernel, which needs a 16-byte aligned input: for an execute whose column
+ * pass input is not aligned, both passes keep the plain layout. */
+static int blk4_usable(const fz_plan *pl, void *const *buf)
+{
+    for (int i = 0; i < pl->npass; i++)
+        if (!pl->pass[i].is_elem && (pl->pass[i].k.flags & FFTZ_F_BLK4_OUT) &&
+            (((uintptr_t)buf[pl->pass[i].src] + (uintptr_t)pl->pass[i].in_off) & 15) != 0)
+            return 0;
+    return 1;
+}
+
 static int launch_passes(fz_plan *ch, void *in, void *out, void *scratch, cudaStream_t st)
 {
     void *buf[FZ_NBUF];
@@ -518,6 +530,7 @@ static int launch_passes(fz_plan *ch, void *in, void *out, void *scratch, cudaSt
         buf[FZ_BUF_SCR0 + i] = (unsigned char *)scratch + off;
         off += (ch->scratch_elems[i] * 2 * (ch->dtype == 0 ? 4 : 8) + 255) & ~(int64_t)255;
     }
+    const int blk = blk4_usable(ch, buf);
     for (int i = 0; i < ch->npass; i++)
     {
         int e;
@@ -533,6 +546,7 @@ static int launch_passes(fz_plan *ch, void *in, void *out, void *scratch, cudaSt
             fftz_pass_t k = ch->pass[i].k;
             k.in = (const unsigned char *)buf[ch->pass[i].src] + ch->pass[i].in_off;
             k.out = (unsigned char *)buf[ch->pass[i].dst] + ch->pass[i].out_off;
+            if (!blk) k.flags &= ~(FFTZ_F_BLK4_IN | FFTZ_F_BLK4_OUT);
             e = fftz_launch_pass(&k, st);
         }
         if (e) return e;
@@ -678,6 +692,7 @@ static aoclfftz_error_type run_on_device(fz_plan *pl, void *in, void *out)
             off += (pl->scratch_elems[i] * 2 * (pl->dtype == 0 ? 4 : 8) + 255) & ~(int64_t)255;
         }
     }
+    const int blk = blk4_usable(pl, buf);
     for (int i = 0; i < pl->npass && ret == AOCLFFTZ_SUCCESS; i++)
     {
         cudaEvent_t *ev = NULL;
@@ -700,6 +715,7 @@ static aoclfftz_error_type run_on_device(fz_plan *pl, void *in, void *out)
             k.in = (const unsigned char *)buf[pl->pass[i].src] + pl->pass[i].in_off;
             k.out = (unsigned char *)buf[pl->pass[i].dst] + pl->pass[i].out_off;
             k.test_tx_short = (int32_t)fz_inj_tma_short;
+            if (!blk) k.flags &= ~(FFTZ_F_BLK4_IN | FFTZ_F_BLK4_OUT);
             e = fftz_launch_pass(&k, st);
         }
         if (ev) cudaEventRecord(ev[1], st);
@@ -849,7 +865,8 @@ FFTZ_INT32 aoclfftz_gpu_describe(FFTZ_VOID *handle, FFTZ_CHAR *buf, FFTZ_INT32 l
         w += pl->pass[i].is_elem ? snprintf(buf + w, (size_t)(len - w), " [%s]", pl->pass[i].what)
                                   : snprintf(buf + w, (size_t)(len - w), " [%s tpc=%d tpt=%d%s]", pl->pass[i].what,
                                              pl->pass[i].k.tpc, pl->pass[i].k.tpt,
-                                             pl->pass[i].k.use_tma == 6   ? " tma-split3"
+                                             (pl->pass[i].k.flags & (FFTZ_F_BLK4_IN | FFTZ_F_BLK4_OUT)) ? " blk4 tma-split"
+                                             : pl->pass[i].k.use_tma == 6 ? " tma-split3"
                                              : pl->pass[i].k.use_tma == 5 ? " tma-split2"
                                              : pl->pass[i].k.use_tma == 4 ? " tma-split"
                                              : pl->pass[i].k.use_tma == 3 ? " tma-prefetch"

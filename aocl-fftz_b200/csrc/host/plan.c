@@ -385,12 +385,12 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         return NULL;
     }
     /* kernel_family 7: 4096-point float rows as two radix-64 tensor-core GEMM
-     * stages (split BF16 x 3; less accurate than the FP32 path, on request only) */
+     * stages (three-term BF16 operands, FP32 accuracy; on request only) */
     if (pl->hints.kernel_family == 7 && k->variant == FFTZ_VAR_FAST && n == 4096 && pl->dtype == 0 &&
-        k->in_mode == 0 && ies == 1 && k->ntf % 4 == 0 && (flags & ~(FFTZ_F_CONJ_IN | FFTZ_F_CONJ_OUT)) == 0)
+        k->in_mode == 0 && ies == 1 && k->ntf % 2 == 0 && (flags & ~(FFTZ_F_CONJ_IN | FFTZ_F_CONJ_OUT)) == 0)
     {
         k->variant = FFTZ_VAR_TC;
-        k->tpc = 4;
+        k->tpc = 2;
         k->use_tma = 0;
         k->smem_tw = 0;
         p->off_tw = fz_tc64_tables(&pl->blob);
@@ -541,6 +541,15 @@ static int fourstep_lines(fz_plan *pl, int64_t n, int64_t n1, int64_t n2, int64_
     fz_pass *pb = line_pass(pl, n2, 1, n1 * oes, bb, nb + 1, 1, S, dst, flags & FFTZ_F_CONJ_OUT, 0);
     if (!pb) return -1;
     pb->out_off = out_off;
+    /* 4096 x 4096 on split tiles both ways: the intermediate in 4 x 4 blocks,
+     * so that the column pass writes whole 128-byte lines and the row pass
+     * reads its four rows as one contiguous slab */
+    if (n1 == 4096 && n2 == 4096 && pl->dtype == 0 && pa->k.use_tma == 4 && pb->k.use_tma == 4 &&
+        pa->k.tpc == 4 && pb->k.tpc == 4 && pb->k.in_mode == 0 && pb->k.out_mode == 1 && pb->k.ibs[0] == n2)
+    {
+        pa->k.flags |= FFTZ_F_BLK4_OUT;
+        pb->k.flags |= FFTZ_F_BLK4_IN;
+    }
     return 0;
 }
 

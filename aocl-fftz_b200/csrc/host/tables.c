@@ -292,16 +292,18 @@ static double bf16_value(uint16_t h)
 
 int64_t fz_tc64_tables(fz_blob *b)
 {
-    /* [A_hi | A_lo | W_4096]: the real 128 x 128 matrix of the 64-point DFT
-     * (rows 2k / 2k+1 = re / im of output k, columns 2j / 2j+1 = re / im of
-     * input j: [[C, S], [-S, C]], C = cos(2 pi jk/64), S = sin(2 pi jk/64)) split
-     * as hi + lo in BF16 and placed in the tensor cores' canonical K-major
-     * layout (8 x 16-byte core matrices, K-chunks 128 B apart, 8-row groups
-     * 2048 B apart); then (cos, sin)(2 pi r / 4096) for r < 4096 as floats. */
+    /* [A_hi | A_mid | A_lo | W_4096]: the real 128 x 128 matrix of the
+     * 64-point DFT (rows 2k / 2k+1 = re / im of output k, columns 2j / 2j+1 =
+     * re / im of input j: [[C, S], [-S, C]], C = cos(2 pi jk/64), S =
+     * sin(2 pi jk/64)) formed in FP64, split as hi + mid + lo in BF16 (each
+     * term the rounding of what the earlier ones left) and placed in the
+     * tensor cores' canonical K-major layout (8 x 16-byte core matrices,
+     * K-chunks 128 B apart, 8-row groups 2048 B apart); then
+     * (cos, sin)(2 pi r / 4096) for r < 4096 as floats. */
     const size_t abytes = 128 * 256;
-    int64_t off = fz_blob_reserve(b, 2 * abytes + 4096 * 8);
+    int64_t off = fz_blob_reserve(b, 3 * abytes + 4096 * 8);
     if (off < 0) return -1;
-    unsigned char *hi = b->p + off, *lo = hi + abytes;
+    unsigned char *hi = b->p + off, *mid = hi + abytes, *lo = mid + abytes;
     for (int row = 0; row < 128; row++)
         for (int kk = 0; kk < 128; kk++)
         {
@@ -315,12 +317,15 @@ int64_t fz_tc64_tables(fz_blob *b)
             else
                 f = (kk & 1) == 0 ? -sn : c;
             const uint16_t h = bf16_bits((float)f);
-            const uint16_t l = bf16_bits((float)(f - bf16_value(h)));
+            const double r1 = f - bf16_value(h);
+            const uint16_t m = bf16_bits((float)r1);
+            const uint16_t l = bf16_bits((float)(r1 - bf16_value(m)));
             const size_t o = (size_t)((row >> 3) * 2048 + (kk >> 3) * 128 + (row & 7) * 16 + (kk & 7) * 2);
             memcpy(hi + o, &h, 2);
+            memcpy(mid + o, &m, 2);
             memcpy(lo + o, &l, 2);
         }
-    float *w = (float *)(b->p + off + 2 * abytes);
+    float *w = (float *)(b->p + off + 3 * abytes);
     for (int r = 0; r < 4096; r++)
     {
         double c, ms;

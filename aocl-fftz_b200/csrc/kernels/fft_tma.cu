@@ -376,7 +376,11 @@ __device__ __forceinline__ void rr_store(const fftz_pass_t &P, const typename Cp
   static_assert(NS * 16 == N, "last stage");
   if (col < 0) return;
   const int64_t oes = P.oes;
-  T2 *ob = (T2 *)P.out + obase + (int64_t)j * oes;
+  // blocked intermediate: output k of column col at (k / 4) * 4 oes + 4 col + k % 4
+  // (the column base obase already holds col; outputs j + 256 r keep the stride)
+  const int64_t jo = (P.flags & FFTZ_F_BLK4_OUT) ? (int64_t)(j >> 2) * 4 * oes + (j & 3) + 3 * col
+                                                 : (int64_t)j * oes;
+  T2 *ob = (T2 *)P.out + obase + jo;
   const int64_t st = (int64_t)NS * oes;
   const bool cj = (P.flags & FFTZ_F_CONJ_OUT) != 0;
   T2 w0 = zero2<T2>(), w = zero2<T2>();
@@ -541,6 +545,15 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            int c4, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5, %6}], [%7];" ::"r"(smem_addr(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // Slice offset of the transpose slot for difference d = writer lane ^ reader
 // lane (XOR-linear in d): column tiles ([n0][m_l][col], 32-byte swizzle) and
 // row tiles ([row][m_l][n0], 128-byte swizzle).
@@ -592,9 +605,11 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
   volatile int *abort_flag = (volatile int *)(cnt + 1);
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const int g = (lane >> 3) & 1, l = (lane & 7) | ((lane >> 4) << 3);
+  // MODE 2 (a blocked intermediate read in 4-row slabs) stages like a column tile
+  constexpr int SMODE = MODE == 2 ? 1 : MODE;
   // the group's sub-transform (transform pw, subsequence n0w) and its slice
   int pw, n0w, wb, c, rd0;
-  if (MODE == 1) {
+  if (SMODE == 1) {
     const int a = w & 1;
     n0w = w >> 1;
     pw = 2 * a + g;
@@ -609,7 +624,7 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
     c = (129 * g) ^ (2 * b);
     rd0 = wb + ((l * 16 + 2 * (l & 7) + g) ^ (2 * b));
   }
-  const int u = split_f<MODE>(l) ^ c;
+  const int u = split_f<SMODE>(l) ^ c;
   const int xw = (pw * 16 + n0w) * 128 + (l ^ (4 * ((pw >> 1) & 1) + 8 * ((pw ^ n0w) & 1)));
   // exchange reader: thread (pr, kr) of the output lane map
   const int pr = OMODE == 1 ? (tid & 3) : (tid >> 8);
@@ -637,7 +652,9 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
     mbar_expect_tx(bar, (unsigned)(N * 4 * sizeof(T2) + P.test_tx_short));
 #pragma unroll 1
     for (int s = 0; s < 16; s++) {
-      if (MODE == 1)
+      if (MODE == 2)  // dims (row in slab, m, n0, slab, line)
+        tma_load_5d(stg + s * 1024, &tmap, 0, 16 * s, 0, c0 >> 2, z, bar);
+      else if (MODE == 1)
         tma_load_4d(stg + s * 1024, &tmap, c0, 16 * s, 0, z, bar);
       else
         tma_load_4d(stg + s * 1024, &tmap, 0, 16 * s, c0, z, bar);
@@ -707,10 +724,10 @@ __global__ void __launch_bounds__(1024, 1) fft_tma_split_kernel(const __grid_con
     {
       T2 *wbase = stg + l * 1024 + wb;
 #pragma unroll
-      for (int k = 0; k < 16; k++) wbase[u ^ split_f<MODE>(k)] = v[k];
+      for (int k = 0; k < 16; k++) wbase[u ^ split_f<SMODE>(k)] = v[k];
       __syncwarp();
 #pragma unroll
-      for (int x = 0; x < 16; x++) v[x] = stg[x * 1024 + wb + (u ^ split_f<MODE>(x))];
+      for (int x = 0; x < 16; x++) v[x] = stg[x * 1024 + wb + (u ^ split_f<SMODE>(x))];
     }
     Dft<16>::template apply<T, T2>(v);  // lane l now holds Z[l + 16 k_hi], k_hi = 0..15
     // release the slice; the last warp issues the next tile's copies
@@ -879,6 +896,8 @@ const void *tma_rr_kernel(int dtype, int n, int tw4, int mode) {
 
 template <int XM> const void *split_pick(int tw4, int mode, int omode) {
   using fftz::fft_tma_split_kernel;
+  if (mode == 2)  // blocked input: the four-step's row pass (plain, transposed store)
+    return (XM == 0 && !tw4 && omode == 1) ? (const void *)&fft_tma_split_kernel<float, 4096, 0, 2, 1, 0> : nullptr;
   if (tw4)
     return mode ? (omode ? (const void *)&fft_tma_split_kernel<float, 4096, 1, 1, 1, XM>
                          : (const void *)&fft_tma_split_kernel<float, 4096, 1, 1, 0, XM>)
@@ -896,16 +915,35 @@ int launch_split(const fftz_pass_t *p, void *stream) {
   if (p->n != 4096 || p->dtype != 0 || p->tpc != 4 || p->tpt != 256) return -1;
   if (p->variant != FFTZ_VAR_FAST && p->variant != FFTZ_VAR_FAST_TW4) return -1;
   if (p->in_kind != FFTZ_IN_COMPLEX || p->out_kind != FFTZ_OUT_COMPLEX) return -1;
-  if ((p->flags & ~(FFTZ_F_CONJ_IN | FFTZ_F_CONJ_OUT | FFTZ_F_TW4)) != 0) return -1;
+  if ((p->flags & ~(FFTZ_F_CONJ_IN | FFTZ_F_CONJ_OUT | FFTZ_F_TW4 | FFTZ_F_BLK4_IN | FFTZ_F_BLK4_OUT)) != 0) return -1;
   if (p->nbdims < 1 || p->nbdims > 2 || p->ind_in || p->ind_out) return -1;
   const int64_t b0 = p->bdim[0], b1 = p->nbdims == 2 ? p->bdim[1] : 1;
   if (b0 % 4 || p->ntf != b0 * b1 || b0 > 0x7fffffff || b1 > 0x7fffffff) return -1;
   if (((uintptr_t)p->in & 15) != 0 || !encoder()) return -1;
-  const int mode = p->in_mode, omode = p->out_mode;
-  cuuint64_t dims[4], strides[3];
-  cuuint32_t box[4], estr[4] = {1, 1, 1, 1};
+  const int blk_in = (p->flags & FFTZ_F_BLK4_IN) != 0;
+  const int mode = blk_in ? 2 : p->in_mode, omode = p->out_mode;
+  cuuint64_t dims[5], strides[4];
+  cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
   CUtensorMapSwizzle swz;
-  if (mode == 1) {
+  int rank = 4;
+  if (mode == 2) {
+    /* blocked rows: element e = n0 + 16 m of row 4 K + r at K * 4 n + 4 e + r
+     * past the line: dims (r, m, n0, K, line) */
+    if (p->ies != 1 || p->ibs[0] != 4096) return -1;
+    dims[0] = 4;
+    dims[1] = 256;
+    dims[2] = 16;
+    dims[3] = (cuuint64_t)(b0 / 4);
+    strides[0] = 64 * 8;
+    strides[1] = 4 * 8;
+    strides[2] = (cuuint64_t)4 * 4096 * 8;
+    box[0] = 4;
+    box[1] = 16;
+    box[2] = 16;
+    box[3] = 1;
+    swz = CU_TENSOR_MAP_SWIZZLE_32B;
+    rank = 5;
+  } else if (mode == 1) {
     /* element e = n0 + 16 m of column c: dims (c, m, n0, outer batch) */
     if (p->ibs[0] != 1 || p->ies <= 0) return -1;
     dims[0] = (cuuint64_t)b0;
@@ -930,14 +968,20 @@ int launch_split(const fftz_pass_t *p, void *stream) {
     box[2] = 4;
     swz = CU_TENSOR_MAP_SWIZZLE_128B;
   }
-  dims[3] = (cuuint64_t)b1;
-  box[3] = 1;
-  strides[2] = p->nbdims == 2 ? (cuuint64_t)(p->ibs[1] * 8) : (cuuint64_t)(4096 * 8 * (mode == 1 ? p->ies : 1));
+  if (mode == 2) {
+    dims[4] = (cuuint64_t)b1;
+    box[4] = 1;
+    strides[3] = p->nbdims == 2 ? (cuuint64_t)(p->ibs[1] * 8) : (cuuint64_t)b0 * 4096 * 8;
+  } else {
+    dims[3] = (cuuint64_t)b1;
+    box[3] = 1;
+    strides[2] = p->nbdims == 2 ? (cuuint64_t)(p->ibs[1] * 8) : (cuuint64_t)(4096 * 8 * (mode == 1 ? p->ies : 1));
+  }
   if (p->nbdims == 2 && p->ibs[1] <= 0) return -1;
-  for (int i = 0; i < 3; i++)
+  for (int i = 0; i < rank - 1; i++)
     if (strides[i] % 16 || strides[i] >= (1ULL << 40)) return -1;
   CUtensorMap map;
-  if (g_encode(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, (void *)p->in, dims, strides, box, estr,
+  if (g_encode(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)rank, (void *)p->in, dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return -1;
@@ -946,6 +990,7 @@ int launch_split(const fftz_pass_t *p, void *stream) {
   const void *fn = xm == 1 ? split_pick<1>(tw4, mode, omode)
                  : xm == 2 ? split_pick<2>(tw4, mode, omode)
                            : split_pick<0>(tw4, mode, omode);
+  if (!fn) return -1;
   const size_t smem = (size_t)fftz::kSplitSmem + (xm == 1 ? fftz::kSplitStash : 16) + 1024;
   static const void *opted[64][32];
   static int nopted[64], nsm[64];
@@ -994,6 +1039,9 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
     const int e = launch_split(p, stream);
     if (e >= 0) return e;
   }
+  /* only the split kernels read or write the blocked intermediate (the host
+   * drops the layout for an execute that cannot take them) */
+  if (p->flags & (FFTZ_F_BLK4_IN | FFTZ_F_BLK4_OUT)) return (int)cudaErrorNotSupported;
   const int tw4 = p->variant == FFTZ_VAR_FAST_TW4;
   int rr = p->use_tma >= 3 && p->tpc * p->tpt <= 1024;
   const void *fn = rr ? tma_rr_kernel(p->dtype, p->n, tw4, mode) : nullptr;

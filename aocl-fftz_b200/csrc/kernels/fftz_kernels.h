@@ -63,6 +63,10 @@ enum fftz_out_kind {
 #define FFTZ_F_POST_TAB   0x10 /* multiply stored value k by post_tab[k*post_es + col*post_cs] */
 #define FFTZ_F_SCALE      0x20 /* multiply stored value by scale                  */
 #define FFTZ_F_MID_TAB    0x40 /* two sweeps: between them v = conj(v) * mid_tab[e] */
+/* 4 x 4 blocked intermediate of a 4096 x 4096 four-step (split kernels only):
+ * element k of column c at (k / 4) * 4 * ncols + 4 * c + k % 4 past the line */
+#define FFTZ_F_BLK4_OUT   0x80  /* the pass writes its output blocked */
+#define FFTZ_F_BLK4_IN    0x100 /* the pass reads its input blocked (rows = k) */
 
 typedef struct fftz_pass
 {

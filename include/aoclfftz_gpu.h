@@ -60,11 +60,16 @@ FFTZ_INT32 aoclfftz_gpu_pass_info(FFTZ_VOID *handle, FFTZ_INT32 i, FFTZ_CHAR *bu
  *                 fetched by TMA copies wherever the pass qualifies
  *                 (0 = choose: TMA copies for column passes); 6 persistent CTAs,
  *                 half of the next tile prefetched by TMA; 7 4096-point float
- *                 row passes as tensor-core GEMM stages (split BF16 x 3: about
- *                 1e-5 relative error, above the FP32 path's bound); 8 every
+ *                 row passes as tensor-core GEMM stages (three-term BF16
+ *                 operands, FP32 accuracy); 8 every
  *                 4096-point float pass as persistent CTAs that keep the tile
- *                 in registers and prefetch the whole next tile by TMA (0 =
- *                 choose takes it for such passes with a column lane map)
+ *                 in registers and prefetch the whole next tile by TMA; 9
+ *                 every 4096-point float pass as 16 x 256 split tiles
+ *                 (persistent, one exchange across the CTA per tile; 0 =
+ *                 choose takes them for such passes with a column lane map);
+ *                 10 / 11 the split tiles with a full-complex exchange and a
+ *                 shared-memory / tensor-memory stash; 12 the in-place
+ *                 runtime-radix kernel instead of the ping-pong tiles
  *   twiddles      where the stage twiddles are read from (see the field)
  * aoclfftz_gpu_set_hints(NULL) restores the defaults. */
 typedef struct aoclfftz_gpu_hints

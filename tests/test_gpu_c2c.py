@@ -270,3 +270,39 @@ def test_split_tiles(family, tag, n, batch, want):
             assert plan.count(tag + "]") == want, plan
     finally:
         lib.aoclfftz_gpu_set_hints(None)
+
+
+def test_blocked_fourstep_intermediate_and_unaligned_input():
+    """The 2^24 four-step on split tiles keeps its intermediate in 4 x 4
+    blocks (both passes marked blk4). An execute whose input is 8 bytes off a
+    16-byte boundary cannot feed the column pass by TMA: it runs both passes
+    on the plain layout instead, with the same result. Both against the FP64
+    oracle."""
+    import torch
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi
+    lib = aoclfftz_b200.load()
+    n = 1 << 24
+    x = synthetic.complex_uniform(9, n, np.complex64)
+    ref = oracle.fft(x.astype(np.complex128))
+    din = torch.zeros(2 * n + 2, dtype=torch.float32, device="cuda")
+    dout = torch.zeros(2 * n, dtype=torch.float32, device="cuda")
+    desc, keep = abi.make_desc(din.data_ptr(), dout.data_ptr(), [(n, 1, 1)], [(1, n, n)], 0, 0, 1)
+    h = abi.setup(lib, desc, "f32")
+    assert h, lib.aoclfftz_gpu_last_error()
+    try:
+        txt = C.create_string_buffer(2048)
+        lib.aoclfftz_gpu_describe(h, txt, 2048)
+        assert txt.value.count(b"blk4") == 2, txt.value
+        for off in (0, 2):  # floats: 0 aligned, 2 = 8 bytes off
+            din.zero_()
+            din[off:off + 2 * n] = torch.from_numpy(x.view(np.float32)).to("cuda")
+            dout.zero_()
+            rc = lib.aoclfftz_execute_io(h, C.c_void_p(din.data_ptr() + 4 * off), C.c_void_p(dout.data_ptr()))
+            assert rc == 0, lib.aoclfftz_gpu_last_error()
+            assert lib.aoclfftz_gpu_synchronize(h) == 0
+            y = dout.cpu().numpy().view(np.complex64)
+            err = oracle.rel_l2(y, ref)
+            assert err <= oracle.tol(n, "f32"), (off, err)
+    finally:
+        lib.aoclfftz_destroy(h)

@@ -1,11 +1,10 @@
 """Tensor-core form (kernel family 7): 4096-point float rows computed as two
-radix-64 DFT-GEMM stages on tcgen05 with split BF16 x 3 operands and FP32
-accumulation.
+radix-64 DFT-GEMM stages on tcgen05 with FP32 accumulation, each operand split
+into three BF16 terms (24 significant bits) and six products per stage.
 
-This form is less accurate than the FP32 SIMT path (a split BF16 x 3 product
-keeps about 16 bits), so it is checked against the FP64 oracle with its own
-bound, rel-L2 <= 1e-4, and its error is reported next to the SIMT path's on the
-same input; the planner never picks it unless asked."""
+Held to the FP32 path's bound against the FP64 oracle: rel-L2 <= 4 log2(N)
+eps_f32 (N = 4096 and the 2^24 four-step line); its error is printed next to
+the SIMT path's on the same input. The planner never picks it unless asked."""
 import ctypes as C
 
 import numpy as np
@@ -18,7 +17,6 @@ from fftz_helpers import cplx_dtype, run_gpu
 
 pytestmark = pytest.mark.gpu
 
-TC_BOUND = 1e-4
 
 
 def _run(family, n, batch, direction, seed):
@@ -45,7 +43,7 @@ def test_tc_rows_4096(direction, batch):
     _, y32, _ = _run(0, 4096, batch, direction, 11 + batch)
     err32 = oracle.rel_l2(y32, ref)
     print("rel-L2 vs FP64 oracle: tensor-core %.3e, FP32 SIMT %.3e" % (err, err32))
-    assert err <= TC_BOUND, err
+    assert err <= oracle.tol(4096, "f32"), err
     assert err32 <= oracle.tol(4096, "f32")
 
 
@@ -58,4 +56,4 @@ def test_tc_fourstep_row_pass():
     ref = oracle.fft(x.astype(np.complex128), sign=-1)
     err = oracle.rel_l2(y, ref)
     print("four-step 2^24 with tensor-core row pass: rel-L2 %.3e" % err)
-    assert err <= TC_BOUND, err
+    assert err <= oracle.tol(n, "f32"), err

@@ -197,3 +197,24 @@ def test_one_component_writer_bases():
                 s4 = 16 * (sw1 >> 4)
                 for kh in range(16):
                     assert exch_real(pw, n0w, l + 16 * kh) == ((xfw - s4) if kh & 1 else (xfw + s4)) + 16 * kh
+
+
+def test_blocked_intermediate_addresses_agree():
+    """The 4096 x 4096 four-step's blocked intermediate: the column pass
+    stores output k1 of column j2 at obase + jo + 256 r * oes (rr_store,
+    k1 = j + 256 r, obase = line * n + j2, jo = (j >> 2) 4 oes + (j & 3) + 3 j2),
+    the row pass's tensor map reads element e of row k1 = 4 K + rr through
+    dims (rr, m, n0, K) with strides (1, 64, 4, 4 n2) elements (e = n0 + 16 m);
+    both must be the same bijection onto [0, n)."""
+    n1 = n2 = 4096
+    oes = n2
+    j2 = np.arange(n2)[:, None]
+    k1 = np.arange(n1)[None, :]
+    j, r = k1 % 256, k1 // 256
+    store = (j2 + (j >> 2) * 4 * oes + (j & 3) + 3 * j2) + 256 * r * oes
+    K, rr = k1 // 4, k1 % 4
+    e = j2
+    n0, m = e % 16, e // 16
+    load = rr * 1 + m * 64 + n0 * 4 + K * 4 * n2
+    assert (store == load).all()
+    assert len(np.unique(store)) == n1 * n2 and store.min() == 0 and store.max() == n1 * n2 - 1

@@ -12,8 +12,9 @@ depends on the selector: every candidate computes the same transform.
 
 The reference's counterpart is a fixed op-count cost model
 (core/solvers/solver.c:124-140) and an unimplemented auto-tuner stub
-(selector/selector.c:989-1004); the "method without the network" here is the
-planner's default choice.
+(selector/selector.c:989-1004). Two "methods without the network" stand
+beside the MLP: the planner's default choice, and that op-count model
+restated over each candidate's passes (opcount_cost).
 """
 import ctypes as C
 import math
@@ -113,6 +114,8 @@ CANDIDATES = [
     dict(kernel_family=5),                    # TMA-fed tiles wherever they qualify
     dict(fourstep_n1=256), dict(fourstep_n1=1024), dict(fourstep_n1=4096),
     dict(algorithm=2),                        # force a four-step split where possible
+    dict(kernel_family=9),                    # 16 x 256 split tiles for every 4096-point float pass
+    dict(kernel_family=12),                   # in-place runtime-radix kernel instead of ping-pong tiles
 ]
 
 
@@ -124,10 +127,15 @@ def _hints(h):
 
 
 def plan_shape(lib, h):
-    """(npass, kinds, per-pass (n, ntf, tpc) summary) parsed from the plan description."""
+    """(plan text, per-pass (kind, n, ntf, tpc)) parsed from the plan description."""
     buf = C.create_string_buffer(4096)
     lib.aoclfftz_gpu_describe(h, buf, 4096)
     text = buf.value.decode()
+    return text, plan_shape_from_text(text)
+
+
+def plan_shape_from_text(text):
+    """Per-pass (kind, n, ntf, tpc) of a plan description."""
     passes = []
     for seg in text.split("[")[1:]:
         seg = seg.split("]")[0]
@@ -141,18 +149,26 @@ def plan_shape(lib, h):
             elif t.startswith("x"):
                 kv["x"] = t[1:]
         passes.append((kind, int(kv.get("n", "1")), int(kv.get("x", "1")), int(kv.get("tpc", "1"))))
-    return text, passes
+    return passes
 
 
 KINDS = ["fast", "pipe", "generic", "bluestein", "elem", "r2c", "c2r"]
-NFEAT = 24
+NBASE = 24  # plan-structure features
+
+
+def cand_onehot(index, ncand=None):
+    """One-hot of the candidate's hint set: candidates whose plans share the
+    same pass structure (TMA use, kernel family) differ only here."""
+    v = np.zeros(ncand or len(CANDIDATES), dtype=np.float32)
+    v[index] = 1.0
+    return v
 
 
 def features(p, passes):
     """Feature vector of one candidate plan of problem p."""
     dims = p["dims"]
     total = float(np.prod(dims))
-    f = np.zeros(NFEAT, dtype=np.float32)
+    f = np.zeros(NBASE, dtype=np.float32)
     f[0] = math.log2(total)
     f[1] = math.log2(p["batch"])
     for k in range(3):
@@ -175,6 +191,70 @@ def features(p, passes):
         f[22] = math.log2(sum(max(n, 1) * max(x, 1) for _, n, x, _ in passes))
     f[23] = math.log2(total * p["batch"]) + (3.0 if p["dtype"] == "f64" else 2.0)
     return f
+
+
+# Cycle weights of the reference's op-count model (api/aoclfftz_internal.h:201-206).
+_W_FMA, _W_MUL, _W_ADD = 4, 3, 1
+
+
+def _radices(n):
+    """The stage radices the planner uses for a line of length n: 16s (then
+    8, 4 or 2) for powers of two, else the balanced power-of-two part and the
+    odd factors (csrc/host/plan.c generic_radices)."""
+    if n <= 1:
+        return []
+    if n & (n - 1) == 0:
+        out, k = [], n.bit_length() - 1
+        st = (k + 3) // 4
+        base, extra = k // st, k % st
+        return [1 << (base + (1 if i < extra else 0)) for i in range(st)]
+    out, k, m = [], 0, n
+    while m % 2 == 0:
+        m //= 2
+        k += 1
+    if k:
+        st = (k + 3) // 4
+        base, extra = k // st, k % st
+        out += [1 << (base + (1 if i < extra else 0)) for i in range(st)]
+    for q in (13, 11, 7, 5, 3):
+        while m % q == 0:
+            out.append(q)
+            m //= q
+    if m != 1:  # Bluestein: count its power-of-two convolution length twice
+        return None
+    return out
+
+
+def _butterfly_ops(R):
+    """Weighted op count of one radix-R butterfly in the reference's scalar
+    model: a split-radix / Winograd-style codelet needs about R log2 R complex
+    additions and (R - 1) twiddle multiplications (4 mul + 2 add each)."""
+    adds = 2 * R * max(1.0, math.log2(R))
+    tw = (R - 1) * (4 * _W_MUL + 2 * _W_ADD)
+    return adds * _W_ADD + tw
+
+
+def opcount_cost(passes):
+    """The reference's fixed cost model (core/solvers/solver.c:124-140:
+    ops = fma*4 + mul*3 + add*1 per codelet call, times the number of calls)
+    restated over a candidate plan's passes: every stage of radix R of a pass
+    of ntf lines of length n calls n / R butterflies per line. It sees the
+    arithmetic only -- not memory traffic, launch shape or kernel family."""
+    cost = 0.0
+    for kind, n, ntf, tpc in passes:
+        if kind.startswith("elem"):
+            cost += 2.0 * n * max(ntf, 1)
+            continue
+        rs = _radices(n)
+        if rs is None:
+            m = 1 << (2 * n - 1).bit_length()
+            rs = _radices(m) or [2]
+            n = m
+            mult = 2.0
+        else:
+            mult = 1.0
+        cost += mult * max(ntf, 1) * sum((n / R) * _butterfly_ops(R) for R in rs)
+    return cost
 
 
 def time_candidates(lib, p, reps=3, candidates=CANDIDATES):
@@ -214,13 +294,15 @@ def time_candidates(lib, p, reps=3, candidates=CANDIDATES):
         ms = float(np.median(ts))
         seen[key] = ms
         results.append((hd, text, features(p, passes), ms))
-    return results
+    # network input: plan structure, then the candidate's one-hot
+    return [(hd, text, np.concatenate([f, cand_onehot(candidates.index(hd), len(candidates))]), ms)
+            for hd, text, f, ms in results]
 
 
 class MLPSelector:
     """The 2 x 64 network, trained on the GPU by aoclfftz_gpu_mlp_* kernels."""
 
-    def __init__(self, lib, nfeat=NFEAT, seed=0):
+    def __init__(self, lib, nfeat=NBASE + len(CANDIDATES), seed=0):
         import torch
         self.lib = lib
         self.F = nfeat
@@ -288,18 +370,77 @@ class MLPSelector:
         return y.cpu().numpy()
 
 
-def regret_report(selector, dataset):
+def regret_report(selector, dataset, opcosts=None):
     """dataset: list of candidate lists (hints, text, features, ms) per
-    problem. Regret = t(chosen) / t(best) - 1 for the network and for the
-    planner's default (the first candidate)."""
-    reg_mlp, reg_def = [], []
-    for cands in dataset:
+    problem, the planner's default first. Regret = t(chosen) / t(best) - 1 for
+    the network, for the planner's default and -- given per-candidate op
+    costs -- for the reference's op-count model (ties keep the earlier
+    candidate, so an indifferent model falls back to the default)."""
+    reg_mlp, reg_def, reg_op = [], [], []
+    for i, cands in enumerate(dataset):
         ms = np.array([c[3] for c in cands])
         best = ms.min()
         pred = selector.predict(np.stack([c[2] for c in cands]))
         reg_mlp.append(ms[int(np.argmin(pred))] / best - 1.0)
         reg_def.append(ms[0] / best - 1.0)
+        if opcosts is not None:
+            reg_op.append(ms[int(np.argmin(np.asarray(opcosts[i])))] / best - 1.0)
     reg_mlp, reg_def = np.array(reg_mlp), np.array(reg_def)
-    return {"problems": len(dataset),
-            "mlp_regret_mean": float(reg_mlp.mean()), "mlp_regret_p95": float(np.percentile(reg_mlp, 95)),
-            "default_regret_mean": float(reg_def.mean()), "default_regret_p95": float(np.percentile(reg_def, 95))}
+    rep = {"problems": len(dataset),
+           "mlp_regret_mean": float(reg_mlp.mean()), "mlp_regret_p95": float(np.percentile(reg_mlp, 95)),
+           "default_regret_mean": float(reg_def.mean()), "default_regret_p95": float(np.percentile(reg_def, 95))}
+    if opcosts is not None:
+        reg_op = np.array(reg_op)
+        rep["opcount_regret_mean"] = float(reg_op.mean())
+        rep["opcount_regret_p95"] = float(np.percentile(reg_op, 95))
+    return rep
+
+
+def load_timings(path):
+    """Autotuner timing database (tests/golden/make_selector_db.py): per
+    problem the candidate rows (default plan first). Returns
+    (train, test, train_opcost, test_opcost): lists of candidate lists
+    (None, None, features, ms) and of per-candidate op costs (None when the
+    database has none). Databases without a split field keep the first 80% of
+    their problems for training."""
+    d = np.load(path)
+    prob, feats, ms = d["problem"], d["features"], d["ms"]
+    if "cand" in d.files:  # the stored rows hold the plan-structure part only
+        feats = np.concatenate([feats, np.eye(len(CANDIDATES), dtype=np.float32)[d["cand"]]], axis=1)
+    opc = d["opcost"] if "opcost" in d.files else None
+    split = d["split"] if "split" in d.files else None
+    order = np.argsort(prob, kind="stable")
+    groups, costs, gsplit = [], [], []
+    cur = -1
+    for k in order:
+        if prob[k] != cur:
+            cur = prob[k]
+            groups.append([])
+            costs.append([])
+            gsplit.append(int(split[k]) if split is not None else -1)
+        groups[-1].append((None, None, feats[k], float(ms[k])))
+        costs[-1].append(float(opc[k]) if opc is not None else 0.0)
+    if split is None:
+        ntrain = int(0.8 * len(groups))
+        gsplit = [0] * ntrain + [1] * (len(groups) - ntrain)
+    tr = [i for i, s_ in enumerate(gsplit) if s_ == 0]
+    te = [i for i, s_ in enumerate(gsplit) if s_ == 1]
+    pick = lambda idx, arr: [arr[i] for i in idx]  # noqa: E731
+    oc = opc is not None
+    return (pick(tr, groups), pick(te, groups), pick(tr, costs) if oc else None, pick(te, costs) if oc else None)
+
+
+def train_and_evaluate(lib, path, epochs=60, seed=0):
+    """Trains the MLP on the database's training problems (log microseconds
+    per candidate) and reports held-out regret of the network, the planner's
+    default and the op-count model against the exhaustive optimum."""
+    train, test, _, test_oc = load_timings(path)
+    X = np.stack([c[2] for g in train for c in g])
+    y = np.log(np.array([c[3] for g in train for c in g]) * 1e3)
+    sel = MLPSelector(lib, nfeat=X.shape[1], seed=seed)
+    hist = sel.fit(X, y, epochs=epochs)
+    rep = regret_report(sel, test, test_oc)
+    rep["train_problems"] = len(train)
+    rep["train_rows"] = int(X.shape[0])
+    rep["loss_first"], rep["loss_last"] = float(hist[0]), float(hist[-1])
+    return sel, rep

@@ -30,7 +30,6 @@ import math
 import os
 import subprocess
 import sys
-import tempfile
 import threading
 import time
 
@@ -45,10 +44,11 @@ WORKLOADS = {
     "ragged": dict(n=0, batch=4096, dtype="f32", ragged=True,
                    desc="ragged batch of 4096 c2c fp32 transforms, lengths log-uniform in [2, 65536] "
                         "(pow2 / 7-smooth / prime thirds), packed, one persistent launch under a CUDA graph, fwd+bwd"),
-    "selector": dict(n=0, batch=2500, dtype="mixed", selector=True,
+    "selector": dict(n=0, batch=0, dtype="mixed", selector=True,
                      desc="learned plan selector: seeded problems (rank 1-3, pow2 / 7-smooth / prime dims, "
-                          "c2c/r2c/c2r, f32/f64, unit or strided, batch 1-256, <= 2^22 elements); candidates "
-                          "timed by the autotuner; 2x64 MLP trained on 80% of problems, regret on the rest"),
+                          "c2c/r2c/c2r, f32/f64, unit or strided, batch 1-256, <= 2^22 elements); 2x64 MLP "
+                          "trained on the autotuner timings of 20000 problems, regret against exhaustive "
+                          "autotuning on 2000 held-out problems (and on fresh problems timed live)"),
     "mixed1000": dict(n=1000, batch=32768, dtype="f32",
                       desc="c2c fp32 N=1000 (2^3 5^3, mixed radix) batch 32768, out-of-place, fwd+bwd"),
     "real3d512": dict(n=512 ** 3, batch=1, dtype="f64", real3d=(512, 512, 512),
@@ -81,8 +81,8 @@ def parse():
     ap.add_argument("--twiddles", type=int, default=0, help="planner hint: 1 global, 2 shared-memory stage twiddles")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--selector-db", default="", help="where --workload selector writes its timing database "
-                                                      "(default: the system temporary directory)")
+    ap.add_argument("--selector-db", default="", help="autotuner timing database of --workload selector "
+                                                      "(default: tests/golden/selector_timings.npz)")
     return ap.parse_args()
 
 
@@ -754,8 +754,13 @@ def run_ragged(args, wl):
 
 
 def run_selector(args, wl):
-    """Autotuner timings -> MLP trained on the GPU -> held-out regret against
-    exhaustive search, next to the planner's default choice."""
+    """Learned plan selector: the MLP trained on the GPU by the library's own
+    kernels on the committed autotuner timings of the training problems
+    (tests/golden/selector_timings.npz, made by make_selector_db.py), regret
+    against exhaustive autotuning on the held-out problems next to the
+    planner's default and the reference's op-count model; plus `--batch` fresh
+    problems (default 50) autotuned live on this GPU and judged with the same
+    network."""
     import numpy as np
     import torch
 
@@ -765,41 +770,24 @@ def run_selector(args, wl):
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     lib = aoclfftz_b200.load()
-    nprob = wl["batch"]
-    probs = selector.random_problems(20261203, nprob)
-    t0 = time.perf_counter()
-    data = []
-    for p in probs:
-        c = selector.time_candidates(lib, p)
-        if len(c) >= 1:
-            data.append((p, c))
-    tune_s = time.perf_counter() - t0
-    ntrain = int(0.8 * len(data))
-    train, test = data[:ntrain], data[ntrain:]
-    X = np.stack([f for _, cs in train for (_, _, f, _) in cs])
-    y = np.log(np.array([ms for _, cs in train for (_, _, _, ms) in cs]) * 1e3)  # log microseconds
-    sel = selector.MLPSelector(lib)
+    db = args.selector_db or os.path.join(ROOT, "tests", "golden", "selector_timings.npz")
     t1 = time.perf_counter()
-    hist = sel.fit(X, y, epochs=args.steps * 10)
+    sel, rep = selector.train_and_evaluate(lib, db, epochs=40)
     fit_s = time.perf_counter() - t1
-    rep = selector.regret_report(sel, [cs for _, cs in test])
-    rep_train = selector.regret_report(sel, [cs for _, cs in train])
-    db = args.selector_db or os.path.join(tempfile.gettempdir(), "aoclfftz_selector_db.npz")
-    os.makedirs(os.path.dirname(os.path.abspath(db)), exist_ok=True)
-    flat = [(i, j, cs[j][2], cs[j][3], json.dumps(cs[j][0])) for i, (_, cs) in enumerate(data) for j in range(len(cs))]
-    np.savez_compressed(db,
-                        problem=np.array([a for a, _, _, _, _ in flat]), cand=np.array([b for _, b, _, _, _ in flat]),
-                        features=np.stack([f for _, _, f, _, _ in flat]), ms=np.array([m for _, _, _, m, _ in flat]),
-                        hints=np.array([h for _, _, _, _, h in flat]),
-                        problems=np.frombuffer(json.dumps([p for p, _ in data]).encode(), dtype=np.uint8))
+    nlive = args.batch if args.batch > 0 else 50
+    t0 = time.perf_counter()
+    live = [selector.time_candidates(lib, p, reps=5) for p in selector.random_problems(20261205, nlive)]
+    live = [[c for c in cs] for cs in live if cs]
+    tune_s = time.perf_counter() - t0
+    live_oc = [[selector.opcount_cost(selector.plan_shape_from_text(c[1])) for c in cs] for cs in live]
+    rep_live = selector.regret_report(sel, live, live_oc)
     value = 100.0 * max(0.0, 1.0 - rep["mlp_regret_mean"])
     return dict(ms=fit_s * 1e3, value=value, hbm_gbs=0.0, rt_err=None, clocks={"sm_mhz": None, "sm_max_mhz": None,
                                                                                 "reasons": ["not sampled"]},
                 launches=0,
-                extra={"selector": dict(rep, train=rep_train, problems_timed=len(data), train_problems=ntrain,
-                                        candidates_per_problem=float(np.mean([len(cs) for _, cs in data])),
-                                        autotune_s=round(tune_s, 1), fit_s=round(fit_s, 2),
-                                        loss_first=float(hist[0]), loss_last=float(hist[-1]))})
+                extra={"selector": dict(rep, database=os.path.relpath(db, ROOT), fit_s=round(fit_s, 2)),
+                       "selector_live": dict(rep_live, problems_timed=len(live), autotune_s=round(tune_s, 1),
+                                             seed=20261205)})
 
 
 def time_reference(wl, threads, transforms, steps, warmup, min_time=None):

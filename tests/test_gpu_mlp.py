@@ -86,19 +86,14 @@ DB = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "selecto
 
 
 @pytest.mark.skipif(not os.path.exists(DB), reason="no autotuner timing database committed")
-def test_learned_selector_beats_default_on_held_out():
-    """Trains on 80% of the committed autotuner timings, evaluates regret
-    against exhaustive search on the held-out 20%."""
-    d = np.load(DB)
-    prob, feats, ms = d["problem"], d["features"], d["ms"]
-    nprob = int(prob.max()) + 1
-    groups = [[(None, None, feats[k], float(ms[k])) for k in np.nonzero(prob == i)[0]] for i in range(nprob)]
-    ntrain = int(0.8 * nprob)
-    train, test = groups[:ntrain], groups[ntrain:]
-    X = np.stack([c[2] for g in train for c in g])
-    y = np.log(np.array([c[3] for g in train for c in g]) * 1e3)
-    sel = selector.MLPSelector(_lib(), nfeat=X.shape[1], seed=0)
-    sel.fit(X, y, epochs=120)
-    rep = selector.regret_report(sel, test)
-    assert rep["mlp_regret_mean"] < rep["default_regret_mean"]
-    assert rep["mlp_regret_mean"] < 0.10
+def test_learned_selector_regret_on_held_out():
+    """Trains the network on the committed autotuner timings of the training
+    problems (the library's own MLP kernels on the GPU) and measures regret
+    against exhaustive autotuning on the held-out problems: at most 5% mean,
+    below the planner's default and below the reference's op-count model
+    restated over the candidates (the methods without the network)."""
+    sel, rep = selector.train_and_evaluate(_lib(), DB, epochs=40)
+    assert rep["problems"] >= 2000 and rep["train_problems"] >= 20000, rep
+    assert rep["mlp_regret_mean"] <= 0.05, rep
+    assert rep["mlp_regret_mean"] < rep["default_regret_mean"], rep
+    assert rep["mlp_regret_mean"] < rep["opcount_regret_mean"], rep

@@ -68,7 +68,7 @@ def test_features():
     p = dict(dims=[1024, 8], kind=1, dtype="f64", strided=True, batch=4, direction=0)
     passes = [("r2c n=1024 x32", 512, 32, 4), ("fast n=8 x2052", 8, 2052, 32)]
     f = selector.features(p, passes)
-    assert f.shape == (selector.NFEAT,) and f.dtype == np.float32
+    assert f.shape == (selector.NBASE,) and f.dtype == np.float32
     assert f[0] == pytest.approx(math.log2(8192)) and f[1] == pytest.approx(2.0)
     assert (f[2], f[3], f[4]) == (10.0, 3.0, 0.0) and f[5] == 2
     assert (f[6], f[7], f[8], f[9]) == (1.0, 1.0, 0.0, 1.0)

@@ -86,13 +86,13 @@ def parse():
     return ap.parse_args()
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# default kernels, from one ncu capture of one 2^24-point transform
-# (profiles/fourstep24_rr_passes_ncu.txt: pass A 221.2 MB, pass B 220.5 MB),
-# scaled to a launch over `batch` transforms (the traffic grows with them).
 L2_BYTES = 126 * 1000 * 1000  # B200 L2
 
-TRAFFIC_PER_TRANSFORM = {("fourstep24", 0): 221.2e6, ("fourstep24", 1): 220.5e6}
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# default kernels, from one ncu capture of one 2^24-point transform
+# (profiles/fourstep24_split_passes_ncu.txt: pass A 212.0 MB, pass B 217.3 MB),
+# scaled to a launch over `batch` transforms (the traffic grows with them).
+TRAFFIC_PER_TRANSFORM = {("fourstep24", 0): 212.0e6, ("fourstep24", 1): 217.3e6}
 
 
 def measured_traffic(workload, args, pass_in_direction, batch):

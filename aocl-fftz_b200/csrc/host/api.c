@@ -866,6 +866,7 @@ FFTZ_INT32 aoclfftz_gpu_describe(FFTZ_VOID *handle, FFTZ_CHAR *buf, FFTZ_INT32 l
                                   : snprintf(buf + w, (size_t)(len - w), " [%s tpc=%d tpt=%d%s]", pl->pass[i].what,
                                              pl->pass[i].k.tpc, pl->pass[i].k.tpt,
                                              (pl->pass[i].k.flags & (FFTZ_F_BLK4_IN | FFTZ_F_BLK4_OUT)) ? " blk4 tma-split"
+                                             : pl->pass[i].k.use_tma == 7 ? " tma-stream"
                                              : pl->pass[i].k.use_tma == 6 ? " tma-split3"
                                              : pl->pass[i].k.use_tma == 5 ? " tma-split2"
                                              : pl->pass[i].k.use_tma == 4 ? " tma-split"

@@ -295,6 +295,9 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
         if ((k->variant == FFTZ_VAR_FAST || k->variant == FFTZ_VAR_FAST_TW4) && pl->dtype == 0 && n == 4096 &&
             (fam == 9 || fam == 10 || fam == 11 || (fam == 0 && (k->in_mode == 1 || k->out_mode == 1))))
             k->use_tma = fam == 10 ? 5 : fam == 11 ? 6 : 4;
+        /* persistent streaming row tiles, whole lines by 1-D bulk copies with
+         * the next tile in flight (kernel_family 13) */
+        if (k->variant == FFTZ_VAR_FAST && k->in_mode == 0 && fam == 13) k->use_tma = 7;
         /* stage twiddles copied to shared memory by each CTA (hint twiddles = 2) */
         k->smem_tw = pl->hints.twiddles == 2 && !ragged_mode(pl) && n >= 512;
         if ((tw4 || tabs) && n < 32 && !(variant_bits & 4))
@@ -335,9 +338,9 @@ static fz_pass *line_pass(fz_plan *pl, int64_t n, int64_t ies, int64_t oes, cons
     finish_launch_shape(pl, k, nslots, maxthr);
     /* split tiles hold four transforms: row passes take four per CTA too when
      * whole tiles cover the first batch dimension */
-    if (k->use_tma >= 4 && k->tpc < 4 && pl->hints.tpc_row == 0 && k->nbdims > 0 && k->bdim[0] % 4 == 0)
-        k->tpc = 4;
-    if (k->use_tma >= 4 && k->tpc != 4) k->use_tma = 3; /* no whole tiles: register-resident kernel */
+    const int split = k->use_tma >= 4 && k->use_tma <= 6;
+    if (split && k->tpc < 4 && pl->hints.tpc_row == 0 && k->nbdims > 0 && k->bdim[0] % 4 == 0) k->tpc = 4;
+    if (split && k->tpc != 4) k->use_tma = 3; /* no whole tiles: register-resident kernel */
     if (is_pipe_variant(k->variant) && fftz_pass_smem_bytes(k) > fftz_smem_limit())
     {
         /* two slots do not fit: the one-tile-per-CTA kernel of the same shape */

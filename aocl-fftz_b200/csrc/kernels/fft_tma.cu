@@ -216,6 +216,95 @@ __global__ void __launch_bounds__(ct_lb<T>(), 1) fft_tma_pipe_kernel(const __gri
   }
 }
 
+// ---------------------------------------------------------------- streaming
+//
+// Persistent row kernel for passes over contiguous lines (unit element
+// stride, 16-byte aligned lines): CTA b runs tiles b, b + G, b + 2 G, ...
+// (G = the grid), each tile's lines copied by one 1-D bulk copy per line into
+// one of two slots. The copies of the next tile are in flight while the
+// current one is computed, its stages run in place in its slot (the first
+// stage reads the dense staged lines with the HBM lane map, later stages use
+// the padded layout), the last stage writes HBM, and once every thread is done
+// with the slot it is refilled with the tile two steps ahead. Several CTAs
+// share an SM, so the SM has several tiles' copies in flight at once.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+template <typename T, int N, int FEAT>
+__global__ void __launch_bounds__(ct_lb<T>()) fft_tma_stream_kernel(const __grid_constant__ fftz_pass_t P,
+                                                                   int64_t ntiles) {
+  typedef typename Cplx<T>::type T2;
+  constexpr int NST = ct_nstages(N);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  unsigned char *base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+  const int tpc = P.tpc;
+  const size_t slot_bytes = ((size_t)tpc * P.sstride * sizeof(T2) + 127) & ~(size_t)127;
+  int64_t *s_in = (int64_t *)(base + 2 * slot_bytes);
+  int64_t *s_out = s_in + tpc;
+  int64_t *s_col = s_out + tpc;
+  // one thread: the lines of `tile` into slot sl (line p at p * N, dense)
+  auto issue = [&](int64_t tile, int sl) {
+    mbar_expect_tx(&bar[sl], (unsigned)(tpc * N * sizeof(T2) + P.test_tx_short));
+    for (int p = 0; p < tpc; p++) {
+      int64_t io, oo, col;
+      batch_offsets(P, tile * tpc + p, &io, &oo, &col);
+      bulk_load((T2 *)(base + sl * slot_bytes) + (size_t)p * N, (const T2 *)P.in + io, (unsigned)(N * sizeof(T2)),
+                &bar[sl]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  int64_t tile = blockIdx.x;
+  if (threadIdx.x == 0) {
+    if (tile < ntiles) issue(tile, 0);
+    if (tile + gridDim.x < ntiles) issue(tile + gridDim.x, 1);
+  }
+  for (unsigned it = 0; tile < ntiles; it++, tile += gridDim.x) {
+    const int sl = (int)(it & 1u);
+    for (int p = threadIdx.x; p < tpc; p += blockDim.x) {
+      int64_t io;
+      batch_offsets(P, tile * tpc + p, &io, s_out + p, s_col + p);
+      s_in[p] = (int64_t)p * N;
+    }
+    // bounded wait for this slot's copies (about a second of polling)
+    bool ok = false;
+    for (long i = 0; i < (1L << 22); i++)
+      if (mbar_try_wait(&bar[sl], (it >> 1) & 1u)) {
+        ok = true;
+        break;
+      }
+    if (!__syncthreads_and(ok)) {  // every thread takes the same branch
+      if (threadIdx.x == 0) {
+        atomicExch(&g_tma_wait_failed, 1);
+        // give the copies still in flight (this slot's, and the other slot's
+        // if it was filled) a bounded time to land before the CTA exits
+        for (long i = 0; i < (1L << 22); i++)
+          if (mbar_try_wait(&bar[sl], (it >> 1) & 1u)) break;
+        if (tile + gridDim.x < ntiles)
+          for (long i = 0; i < (1L << 22); i++)
+            if (mbar_try_wait(&bar[sl ^ 1], ((it + 1) >> 1) & 1u)) break;
+      }
+      return;
+    }
+    FastStages<T, N, 0, NST, 0, 1, FEAT, true, 1>::run(P, (T2 *)(base + sl * slot_bytes), s_in, s_out, s_col, 1,
+                                                       nullptr);
+    // every thread is done with the slot and the offsets: refill the slot
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0 && tile + 2 * (int64_t)gridDim.x < ntiles) issue(tile + 2 * (int64_t)gridDim.x, sl);
+  }
+}
+
 // ------------------------------------------------------- register-resident
 //
 // Persistent 4096-point float kernel whose whole next tile is in flight while
@@ -894,6 +983,75 @@ const void *tma_rr_kernel(int dtype, int n, int tw4, int mode) {
 }
 
 
+const void *tma_stream_kernel(int dtype, int n) {
+  using fftz::fft_tma_stream_kernel;
+  if (dtype == 0) switch (n) {
+      case 256: return (const void *)&fft_tma_stream_kernel<float, 256, 0>;
+      case 512: return (const void *)&fft_tma_stream_kernel<float, 512, 0>;
+      case 1024: return (const void *)&fft_tma_stream_kernel<float, 1024, 0>;
+      case 2048: return (const void *)&fft_tma_stream_kernel<float, 2048, 0>;
+      case 4096: return (const void *)&fft_tma_stream_kernel<float, 4096, 0>;
+      case 8192: return (const void *)&fft_tma_stream_kernel<float, 8192, 0>;
+    }
+  else switch (n) {
+      case 256: return (const void *)&fft_tma_stream_kernel<double, 256, 0>;
+      case 512: return (const void *)&fft_tma_stream_kernel<double, 512, 0>;
+      case 1024: return (const void *)&fft_tma_stream_kernel<double, 1024, 0>;
+      case 2048: return (const void *)&fft_tma_stream_kernel<double, 2048, 0>;
+      case 4096: return (const void *)&fft_tma_stream_kernel<double, 4096, 0>;
+    }
+  return nullptr;
+}
+
+/* The streaming row kernel: plain row passes (no epilogue features) over
+ * 16-byte aligned contiguous lines; -1 when the pass does not qualify. */
+int launch_stream(const fftz_pass_t *p, void *stream) {
+  if (p->variant != FFTZ_VAR_FAST || p->in_mode != 0 || p->ies != 1 || p->smem_tw || p->ind_in) return -1;
+  const int64_t esz = p->dtype == 0 ? 8 : 16;
+  if (p->tpc < 1 || p->ntf % p->tpc || ((uintptr_t)p->in & 15) || (p->n * esz) % 16) return -1;
+  for (int d = 0; d < p->nbdims; d++)
+    if ((p->ibs[d] * esz) % 16) return -1;
+  const void *fn = tma_stream_kernel(p->dtype, (int)p->n);
+  if (!fn) return -1;
+  const size_t slot = ((size_t)p->tpc * p->sstride * esz + 127) & ~(size_t)127;
+  const size_t smem = 2 * slot + 3 * 8 * (size_t)p->tpc + 128;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  static const void *opted[64][16];
+  static int nopted[64], maxdyn[64][16];
+  int s = -1;
+  for (int i = 0; i < nopted[dev]; i++)
+    if (opted[dev][i] == fn) s = i;
+  if (s < 0) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) return (int)cudaGetLastError();
+    const int md = (int)(fftz_smem_limit() - (int64_t)fa.sharedSizeBytes);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+    if (e != cudaSuccess) return (int)e;
+    if (nopted[dev] < 16) {
+      s = nopted[dev]++;
+      opted[dev][s] = fn;
+      maxdyn[dev][s] = md;
+    }
+  }
+  if (s < 0 || smem > (size_t)maxdyn[dev][s]) return -1;
+  const dim3 block((unsigned)(p->tpc * p->tpt));
+  int64_t ntiles = p->ntf / p->tpc;
+  if (ntiles <= 0) return 0;
+  static int nsm[64];
+  if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, (int)block.x, smem) != cudaSuccess || occ < 1) {
+    cudaGetLastError();
+    occ = 1;
+  }
+  const int64_t cap = (int64_t)occ * (nsm[dev] > 0 ? nsm[dev] : 148);
+  const dim3 grid((unsigned)(ntiles < cap ? ntiles : cap));
+  void *args[2] = {(void *)p, (void *)&ntiles};
+  return (int)cudaLaunchKernel(fn, grid, block, args, smem, (cudaStream_t)stream);
+}
+
 template <int XM> const void *split_pick(int tw4, int mode, int omode) {
   using fftz::fft_tma_split_kernel;
   if (mode == 2)  // blocked input: the four-step's row pass (plain, transposed store)
@@ -1035,6 +1193,7 @@ int fftz_launch_pass_tma(const fftz_pass_t *p, void *stream) {
   const int64_t b0 = p->bdim[0], b1 = p->nbdims == 2 ? p->bdim[1] : 1;
   if (p->tpc < 1 || b0 % p->tpc || p->ntf != b0 * b1) return -1;
   if (((uintptr_t)p->in & 15) != 0) return -1;
+  if (p->use_tma == 7) return launch_stream(p, stream);
   if (p->use_tma >= 4) {
     const int e = launch_split(p, stream);
     if (e >= 0) return e;

@@ -112,7 +112,9 @@ typedef struct fftz_pass
      * (output) offset instead of i * ibs (i * obs) -- transforms of one length
      * scattered through a packed ragged buffer form one batched pass */
     int32_t ind_dim;
-    int32_t use_tma;                    /* fetch the tile with TMA copies when the pass qualifies */
+    int32_t use_tma;                    /* fetch the tile with TMA copies when the pass qualifies: 1 one
+                                           tile per CTA, 2 half-prefetch, 3 register-resident, 4-6 split
+                                           tiles, 7 streaming rows */
     int32_t smem_tw;                    /* compile-time kernels: copy the stage twiddles to shared memory */
     int32_t test_tx_short;              /* fault injection (tests): TMA tiles expect this many bytes more
                                            than their copies deliver, so the bounded tile wait runs out */

@@ -382,6 +382,35 @@ def run_ours(args, wl):
                         "GB/s": round((p[2] + p[3]) * esz / (t / K * 1e-3) / 1e9, 1)}
                        for p, t in zip(passes, times)])
 
+    # the same bytes moved by plain device copies over the same buffer
+    # rotation (input -> intermediate -> output, as the two directions do):
+    # what a pass of this size can reach, beside the large-copy peak
+    def copy_step():
+        a, b_, c = sets[cur[0]]
+        cur[0] = (cur[0] + 1) % nsets
+        b_.copy_(a)
+        c.copy_(b_)
+
+    cur[0] = 0
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, nsets)):
+            copy_step()
+    torch.cuda.synchronize()
+    c0 = torch.cuda.Event(enable_timing=True)
+    c1 = torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(K):
+            copy_step()
+    c1.record(stream)
+    torch.cuda.synchronize()
+    copy_ms = max_over_ranks(c0.elapsed_time(c1), ws) / K
+    res["copy_ceiling"] = {"ms_per_step": round(copy_ms, 5),
+                           "GB/s": round(2 * 2 * total * esz / (copy_ms * 1e-3) / 1e9, 1),
+                           "fft_step_over_copy_step": round(ms / copy_ms, 3),
+                           "how": "torch device copies of the same bytes (in -> mid -> out per step) over the same "
+                                  "buffer rotation, CUDA events"}
+
     # end to end through the C ABI with pinned host buffers
     if not args.no_e2e:
         hy = torch.empty_like(hx).pin_memory()
@@ -1047,7 +1076,7 @@ def main():
                        "parallelism": "replicas dp%d" % ws},
             "hbm_gbs": round(r["hbm_gbs"], 1), "hbm_frac_of_measured": round(r["hbm_gbs"] / peak, 4),
             "gpu_launches": r["launches"], "clocks": r["clocks"], "round_trip_rel_l2": r["rt_err"]}
-    for key in ("roofline", "passes"):
+    for key in ("roofline", "passes", "copy_ceiling"):
         if key in r:
             line[key] = r[key]
     line.update(r.get("extra", {}))

@@ -69,7 +69,9 @@ FFTZ_INT32 aoclfftz_gpu_pass_info(FFTZ_VOID *handle, FFTZ_INT32 i, FFTZ_CHAR *bu
  *                 choose takes them for such passes with a column lane map);
  *                 10 / 11 the split tiles with a full-complex exchange and a
  *                 shared-memory / tensor-memory stash; 12 the in-place
- *                 runtime-radix kernel instead of the ping-pong tiles
+ *                 runtime-radix kernel instead of the ping-pong tiles; 13
+ *                 row passes of contiguous lines as persistent streaming
+ *                 tiles (whole lines by bulk copies, next tile in flight)
  *   twiddles      where the stage twiddles are read from (see the field)
  * aoclfftz_gpu_set_hints(NULL) restores the defaults. */
 typedef struct aoclfftz_gpu_hints

@@ -272,6 +272,49 @@ def test_split_tiles(family, tag, n, batch, want):
         lib.aoclfftz_gpu_set_hints(None)
 
 
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n,batch,rs", [(4096, 1024, 0), (4096, 37, 0), (1024, 300, 0), (256, 512, 0),
+                                        (8192, 20, 0), (2048, 50, 2), (2048, 50, 1), (1 << 20, 2, 0),
+                                        (1 << 24, 1, 0)])
+def test_streaming_row_tiles(dtype, n, batch, rs):
+    """Kernel family 13: row passes over contiguous lines as persistent
+    streaming tiles (each line by one 1-D bulk copy into one of two slots,
+    the next tile in flight). Rows `rs` elements apart beyond n: 0 dense, 2
+    still 16-byte aligned (f32), 1 not aligned for f32 (the pass runs on the
+    one-tile kernel instead). Four-step sizes run their row pass (transposed
+    store) this way. Against the oracle and the reference, both directions."""
+    if dtype == "f64" and n == 1 << 24:
+        n = 1 << 22
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi
+    lib = aoclfftz_b200.load()
+    h = abi.Hints()
+    h.kernel_family = 13
+    lib.aoclfftz_gpu_set_hints(C.byref(h))
+    try:
+        for d in (0, 1):
+            _, plan = check_c2c(dtype, [(n, 1, 1)], [(batch, n + rs, n + rs)], d, compare_ref=n < (1 << 20))
+            assert "tma-stream" in plan, plan
+    finally:
+        lib.aoclfftz_gpu_set_hints(None)
+
+
+def test_streaming_rows_in_place():
+    """Family 13 in place: every tile is staged before its lines are
+    overwritten; against the oracle."""
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi
+    lib = aoclfftz_b200.load()
+    h = abi.Hints()
+    h.kernel_family = 13
+    lib.aoclfftz_gpu_set_hints(C.byref(h))
+    try:
+        for dtype in ("f32", "f64"):
+            check_c2c(dtype, [(4096, 1, 1)], [(333, 4096, 4096)], 0, placement=0)
+    finally:
+        lib.aoclfftz_gpu_set_hints(None)
+
+
 def test_blocked_fourstep_intermediate_and_unaligned_input():
     """The 2^24 four-step on split tiles keeps its intermediate in 4 x 4
     blocks (both passes marked blk4). An execute whose input is 8 bytes off a

@@ -7,7 +7,7 @@ events and keeps the fastest -- exhaustive search, always correct, costly.
 The learned selector predicts each candidate's log time with a small MLP
 trained on autotuner timings by the library's own CUDA kernels
 (aoclfftz_gpu_mlp_*) and picks the argmin without timing; the exhaustive
-autotuner stays its fallback and the judge of its regret. No transform result
+autotuner stays its fallback and the yardstick of its regret. No transform result
 depends on the selector: every candidate computes the same transform.
 
 The reference's counterpart is a fixed op-count cost model

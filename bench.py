@@ -788,7 +788,7 @@ def run_selector(args, wl):
     (tests/golden/selector_timings.npz, made by make_selector_db.py), regret
     against exhaustive autotuning on the held-out problems next to the
     planner's default and the reference's op-count model; plus `--batch` fresh
-    problems (default 50) autotuned live on this GPU and judged with the same
+    problems (default 50) autotuned live on this GPU and scored with the same
     network."""
     import numpy as np
     import torch

@@ -17,7 +17,10 @@ same step through the public C ABI with pinned host buffers (the library
 stages them: copy in, transform, copy out). `roofline` describes the dominant
 kernel, timed with CUDA events on the plan's stream during the timed region.
 `cpu_baseline` times the reference library (built from its sources, OpenMP)
-on a bounded sample on this host's cores.
+on a bounded sample on this host's cores. `fp64_oracle` states the error of
+the timed run's own forward outputs against the FP64 oracle. `copy_ceiling`
+(c2c workloads) times plain device copies of the same bytes over the same
+buffer rotation: the bandwidth a pass of this size can reach.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU (torchrun, one process per GPU): every rank runs its own batch

@@ -193,8 +193,21 @@ def features(p, passes):
     return f
 
 
-# Cycle weights of the reference's op-count model (api/aoclfftz_internal.h:201-206).
-_W_FMA, _W_MUL, _W_ADD = 4, 3, 1
+# The reference's op-count cost model. Cycle weights of its operation classes
+# (api/aoclfftz_internal.h:201-206): fma, mul, add, move, perm, other.
+_W_OPS = (4, 3, 1, 1, 1, 1)
+# Operation counts (fma, mul, add, move, perm, other) per call of the
+# reference's scalar codelets, as their ops_cnt tables state them: the first
+# stage of a line runs the plain codelet (core/kernels/dft/c2c/c/fft<R>c.c),
+# every later stage the twiddled one
+# (core/kernels/dft/tw_c2c_fwd/c/twid_fwd_fft<R>c.c; the backward tables are
+# the same), for the radices this planner uses.
+_OPS_FIRST = {2: (0, 0, 4, 8, 0, 0), 3: (0, 4, 12, 12, 0, 0), 4: (0, 0, 16, 16, 0, 0), 5: (0, 12, 32, 20, 0, 0),
+              7: (0, 36, 60, 28, 0, 0), 8: (0, 4, 52, 32, 0, 0), 11: (0, 100, 140, 44, 0, 0),
+              13: (0, 68, 176, 52, 0, 0), 16: (0, 24, 144, 64, 0, 0)}
+_OPS_TW = {2: (0, 4, 6, 10, 0, 0), 3: (0, 12, 16, 16, 0, 0), 4: (0, 12, 22, 22, 0, 0), 5: (0, 28, 40, 28, 0, 0),
+           7: (0, 60, 72, 40, 0, 0), 8: (0, 32, 66, 46, 0, 0), 11: (0, 140, 160, 64, 0, 0),
+           13: (0, 116, 200, 76, 0, 0), 16: (0, 84, 174, 94, 0, 0)}
 
 
 def _radices(n):
@@ -225,21 +238,22 @@ def _radices(n):
     return out
 
 
-def _butterfly_ops(R):
-    """Weighted op count of one radix-R butterfly in the reference's scalar
-    model: a split-radix / Winograd-style codelet needs about R log2 R complex
-    additions and (R - 1) twiddle multiplications (4 mul + 2 add each)."""
-    adds = 2 * R * max(1.0, math.log2(R))
-    tw = (R - 1) * (4 * _W_MUL + 2 * _W_ADD)
-    return adds * _W_ADD + tw
+def codelet_cost(R, first):
+    """Weighted cycles of one call of the reference's radix-R codelet (core/
+    solvers/solver.c:124-140: fma * 4 + mul * 3 + add + move + perm + other)."""
+    counts = (_OPS_FIRST if first else _OPS_TW)[R]
+    return sum(w * c for w, c in zip(_W_OPS, counts))
 
 
 def opcount_cost(passes):
-    """The reference's fixed cost model (core/solvers/solver.c:124-140:
-    ops = fma*4 + mul*3 + add*1 per codelet call, times the number of calls)
-    restated over a candidate plan's passes: every stage of radix R of a pass
-    of ntf lines of length n calls n / R butterflies per line. It sees the
-    arithmetic only -- not memory traffic, launch shape or kernel family."""
+    """The reference's fixed cost model restated over a candidate plan's
+    passes: a line of length n with stage radices R_0, R_1, ... calls n / R_s
+    codelets in stage s, the plain codelet in stage 0 and the twiddled one
+    after it, each weighted by its operation counts (codelet_cost); a pass of
+    ntf lines costs ntf times that; a line without a radix split (Bluestein)
+    counts its power-of-two convolution length twice; elementwise passes 2 n
+    per line. It sees the arithmetic only -- not memory traffic, launch shape
+    or kernel family."""
     cost = 0.0
     for kind, n, ntf, tpc in passes:
         if kind.startswith("elem"):
@@ -253,7 +267,7 @@ def opcount_cost(passes):
             mult = 2.0
         else:
             mult = 1.0
-        cost += mult * max(ntf, 1) * sum((n / R) * _butterfly_ops(R) for R in rs)
+        cost += mult * max(ntf, 1) * sum((n // R) * codelet_cost(R, s == 0) for s, R in enumerate(rs))
     return cost
 
 

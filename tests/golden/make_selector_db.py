@@ -22,8 +22,15 @@ plan-structure feature vector, median ms, and the reference-style op-count cost 
 With --partial the run saves its progress every 500 problems and resumes from
 that file; --time-limit stops (after saving) when the limit is reached, so a
 long generation can span several runs.
+
+  python tests/golden/make_selector_db.py --recost IN [--out PATH]
+
+re-plans every stored (problem, candidate) row of database IN (no timing) and
+rewrites its op-count column with the current selector.opcount_cost; every
+other column is kept as it is.
 """
 import argparse
+import ctypes as C
 import json
 import os
 import sys
@@ -75,6 +82,45 @@ def save(path, rows, problems, done):
                         problems=np.frombuffer(json.dumps(problems).encode(), dtype=np.uint8))
 
 
+def recost(path_in, path_out):
+    import torch
+    import aoclfftz_b200
+    from aoclfftz_b200 import abi, selector
+
+    torch.cuda.set_device(0)
+    lib = aoclfftz_b200.load()
+    d = np.load(path_in)
+    problems = json.loads(bytes(d["problems"]).decode())
+    prob, cand = d["problem"], d["cand"]
+    opcost = np.zeros(len(prob), dtype=np.float64)
+    t0 = time.perf_counter()
+    bufs = {}
+    for k in range(len(prob)):
+        p = problems[int(prob[k])]
+        if int(prob[k]) not in bufs:
+            bufs.clear()
+            _, _, in_sc, out_sc = selector.descriptor(p, 1, 2)
+            tdt = torch.float32 if p["dtype"] == "f32" else torch.float64
+            bufs[int(prob[k])] = (torch.zeros(in_sc, dtype=tdt, device="cuda"),
+                                  torch.zeros(out_sc, dtype=tdt, device="cuda"))
+        x, y = bufs[int(prob[k])]
+        lib.aoclfftz_gpu_set_hints(C.byref(selector._hints(selector.CANDIDATES[int(cand[k])])))
+        desc, keep, _, _ = selector.descriptor(p, x.data_ptr(), y.data_ptr())
+        h = abi.setup(lib, desc, p["dtype"])
+        lib.aoclfftz_gpu_set_hints(None)
+        if not h:
+            raise RuntimeError("row %d: %s" % (k, lib.aoclfftz_gpu_last_error().decode()))
+        text, passes = selector.plan_shape(lib, h)
+        lib.aoclfftz_destroy(h)
+        opcost[k] = selector.opcount_cost(passes)
+        if (k + 1) % 20000 == 0:
+            print("%d rows, %.1f s" % (k + 1, time.perf_counter() - t0), flush=True)
+    out = {f: d[f] for f in d.files}
+    out["opcost"] = opcost
+    np.savez_compressed(path_out, **out)
+    print("wrote %s: %d rows re-costed" % (path_out, len(prob)), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=20000)
@@ -82,7 +128,11 @@ def main():
     ap.add_argument("--partial", default="")
     ap.add_argument("--time-limit", type=float, default=0.0)
     ap.add_argument("--out", default=os.path.join(HERE, "selector_timings.npz"))
+    ap.add_argument("--recost", default="")
     args = ap.parse_args()
+    if args.recost:
+        recost(args.recost, args.out)
+        return
     import torch
     import aoclfftz_b200
     from aoclfftz_b200 import selector

@@ -99,3 +99,63 @@ def test_regret_report():
     worst = selector.regret_report(_Stub(lambda X: -X[:, 0]), data)
     assert worst["mlp_regret_mean"] == pytest.approx((3.0 + 2.0 + 1.0) / 3.0)
     assert worst["problems"] == 3
+
+
+def test_codelet_costs_follow_the_reference_tables():
+    """codelet_cost weighs the reference's per-call operation counts (fma,
+    mul, add, move, perm, other) by its cycle weights 4, 3, 1, 1, 1, 1: e.g.
+    the plain radix-16 codelet {0, 24, 144, 64, 0, 0} -> 280, the twiddled
+    one {0, 84, 174, 94, 0, 0} -> 520, the plain radix-2 {0, 0, 4, 8, 0, 0} -> 12."""
+    assert selector.codelet_cost(16, True) == 280
+    assert selector.codelet_cost(16, False) == 520
+    assert selector.codelet_cost(2, True) == 12
+    assert selector.codelet_cost(5, False) == 28 * 3 + 40 + 28
+    for R in (2, 3, 4, 5, 7, 8, 11, 13, 16):
+        # a twiddled call never costs less than the plain one
+        assert selector.codelet_cost(R, False) > selector.codelet_cost(R, True)
+
+
+def test_opcount_cost_of_plans():
+    """Per line: n / R_s calls of stage s's codelet, the plain one first;
+    linear in the number of lines; a line with no radix split (Bluestein)
+    counts its power-of-two convolution twice; elementwise passes 2 n."""
+    c16, t16 = selector.codelet_cost(16, True), selector.codelet_cost(16, False)
+    one = selector.opcount_cost([("fast", 4096, 1, 1)])
+    assert one == 256 * c16 + 2 * 256 * t16
+    assert selector.opcount_cost([("fast", 4096, 7, 1)]) == 7 * one
+    # 1000 = 8 * 5 * 5 * 5
+    c8, t5 = selector.codelet_cost(8, True), selector.codelet_cost(5, False)
+    assert selector.opcount_cost([("generic", 1000, 1, 4)]) == 125 * c8 + 3 * 200 * t5
+    # prime 1009: m = 2048 = 16 * 16 * 8, twice
+    c2048 = 128 * c16 + 128 * t16 + 256 * selector.codelet_cost(8, False)
+    assert selector.opcount_cost([("bluestein", 1009, 3, 1)]) == 2 * 3 * c2048
+    assert selector.opcount_cost([("elem", 500, 4, 1)]) == 2 * 500 * 4
+    # a four-step (two passes) costs more arithmetic than one pass of the same length
+    assert selector.opcount_cost([("fast", 64, 64, 1), ("fast", 64, 64, 1)]) > 0
+
+
+def test_selector_database_layout():
+    """The committed autotuner database: 20000 training and 2000 held-out
+    problems (seeded draws, so a few repeat within a split) whose problem
+    descriptions are disjoint between the splits, every row a distinct plan
+    with its candidate's one-hot, a positive median time and op cost."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "selector_timings.npz")
+    train, test, train_oc, test_oc = selector.load_timings(path)
+    assert len(train) == 20000 and len(test) == 2000
+    nf = selector.NBASE + len(selector.CANDIDATES)
+    for groups, costs in ((train, train_oc), (test, test_oc)):
+        for g, c in zip(groups[:500], costs[:500]):
+            assert len(g) == len(c) >= 1
+            for (_, _, f, ms), oc in zip(g, c):
+                assert f.shape == (nf,) and ms > 0 and oc > 0
+                assert f[selector.NBASE:].sum() == 1.0
+    d = np.load(path)
+    probs = json.loads(bytes(d["problems"]).decode())
+    u, first = np.unique(d["problem"], return_index=True)
+    sp = d["split"][first]
+    assert (sp == 0).sum() == 20000 and (sp == 1).sum() == 2000
+    tr = {json.dumps(probs[i], sort_keys=True) for i in u[sp == 0]}
+    te = {json.dumps(probs[i], sort_keys=True) for i in u[sp == 1]}
+    assert not (tr & te)

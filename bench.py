@@ -738,6 +738,8 @@ def run_ragged(args, wl):
     time.sleep(0.3)
     ms = timed(step, args.steps)
     clk = clocks.stop()
+    # the timed run's forward outputs, for the FP64 check of the CPU leg
+    yc = dy.view(torch.complex64 if dtype == "f32" else torch.complex128).cpu().numpy().copy()
     # plain path: one ordinary plan per transform, same stream
     plans = []
     t0 = time.perf_counter()
@@ -775,7 +777,7 @@ def run_ragged(args, wl):
             "bytes_per_launch": per_launch, "ms_per_launch": round(ms / 2, 5),
             "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind}
     return dict(ms=ms, value=flops / (ms * 1e-3) / 1e9, hbm_gbs=alg_bytes / (ms * 1e-3) / 1e9, rt_err=rt,
-                buffer_bytes=total * esz,
+                buffer_bytes=total * esz, ragged_check=(sizes, offs, x, yc, dtype),
                 clocks=clk, launches=2 * args.steps, roofline=roof,
                 extra={"plain_path": {"ms_per_step": round(ms_plain, 4),
                                       "value": round(flops / (ms_plain * 1e-3) / 1e9, 2),
@@ -1042,6 +1044,35 @@ def fp64_check(n, dtype, x0, y0, x1, y1):
             "exact_bins_rel_l2": e_bins, "exact_bins": "%d seeded bins of the first and last transform" % len(bins)}
 
 
+def ragged_fp64_check(sizes, offs, x, y, dtype, every=16):
+    """FP64-oracle error of the ragged run's forward outputs: every `every`-th
+    transform of the batch against oracle.fft, each against its own bound
+    4 log2(n) eps of the dtype; reports the sample's overall rel-L2, the worst
+    error / bound ratio and that transform."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    num = den = 0.0
+    worst = (0.0, 0, 0.0, 0.0)
+    idx = list(range(0, len(sizes), every))
+    for i in idx:
+        o, n = int(offs[i]), int(sizes[i])
+        ref = oracle.fft(np.asarray(x[o:o + n], dtype=np.complex128))
+        d = np.asarray(y[o:o + n], dtype=np.complex128) - ref
+        num += float(np.vdot(d, d).real)
+        den += float(np.vdot(ref, ref).real)
+        e = float(oracle.rel_l2(y[o:o + n], ref))
+        b = oracle.tol(n, dtype) if n > 1 else oracle.tol(2, dtype)
+        if e / b > worst[0]:
+            worst = (e / b, n, e, b)
+    return {"rel_l2": math.sqrt(num / max(den, 1e-300)), "worst_err_over_bound": round(float(worst[0]), 4),
+            "worst_transform": {"n": worst[1], "rel_l2": float(worst[2]), "bound": float(worst[3])},
+            "bins": "all bins of every %d-th transform (%d of %d, FP64 fast FFT), each against "
+                    "4 log2(n) eps" % (every, len(idx), len(sizes))}
+
+
 METRIC = "5N·log2N GFLOP/s + HBM GB/s vs plain GPU FFT at stated FP64 err, 1 B200"
 
 
@@ -1093,6 +1124,11 @@ def main():
         if r.get("fwd_check") is not None:
             try:
                 line["fp64_oracle"] = fp64_check(*r["fwd_check"])
+            except Exception as e:
+                line["fp64_oracle"] = {"unavailable": str(e)}
+        if r.get("ragged_check") is not None:
+            try:
+                line["fp64_oracle"] = ragged_fp64_check(*r["ragged_check"])
             except Exception as e:
                 line["fp64_oracle"] = {"unavailable": str(e)}
         try:

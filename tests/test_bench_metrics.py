@@ -63,3 +63,39 @@ def test_measured_traffic_only_for_the_captured_configuration():
     for kw in ({"family": 8}, {"tpc_col": 8}, {"tpc_row": 2}, {"fourstep_n1": 2048}, {"twiddles": 2}):
         assert bench.measured_traffic("fourstep24", _args(**kw), 0, 4) is None
     assert bench.measured_traffic("batch4096", _args(), 0, 1024) is None
+
+
+def test_ragged_fp64_check_measures_each_transform():
+    """The ragged line's FP64 check: exact outputs give errors at the dtype's
+    rounding level; one output bin off by 1e-3 of its transform's norm shows
+    up as that transform's error above its own bound."""
+    import numpy as np
+    sizes = [5, 16, 7, 1, 1024, 97, 2, 331]
+    offs = np.cumsum([0] + sizes[:-1])
+    rng = np.random.default_rng(3)
+    x = (rng.standard_normal(sum(sizes)) + 1j * rng.standard_normal(sum(sizes))).astype(np.complex64)
+    y = np.concatenate([np.fft.fft(x[o:o + n].astype(np.complex128)).astype(np.complex64)
+                        for o, n in zip(offs, sizes)])
+    ok = bench.ragged_fp64_check(sizes, offs, x, y, "f32", every=1)
+    assert ok["rel_l2"] < 1e-6 and ok["worst_err_over_bound"] < 1.0
+    bad = y.copy()
+    o, n = int(offs[5]), sizes[5]
+    bad[o + 3] += 1e-3 * np.linalg.norm(y[o:o + n])
+    res = bench.ragged_fp64_check(sizes, offs, x, bad, "f32", every=1)
+    assert res["worst_transform"]["n"] == 97 and res["worst_err_over_bound"] > 100
+
+
+def test_real3d_fp64_check_against_exact_sums():
+    """The real 3-D line's FP64 check: numpy's FP64 rfftn passes at rounding
+    level; a perturbed bin in the sub-block is caught."""
+    import numpy as np
+    x = np.random.default_rng(4).standard_normal((16, 8, 32))
+    F = np.fft.rfftn(x)
+    k0 = np.arange(0, 17)
+    k1 = (np.arange(8) * 7 + 3) % 8
+    k2 = (np.arange(16) * 11 + 5) % 16
+    got = F[k2][:, k1][:, :, k0]
+    ok = bench.real3d_fp64_check(x, got, k0, k1, k2)
+    assert ok["rel_l2"] < ok["bound"]
+    got[2, 3, 4] += 1e-6 * np.abs(got).max()
+    assert bench.real3d_fp64_check(x, got, k0, k1, k2)["rel_l2"] > ok["bound"]

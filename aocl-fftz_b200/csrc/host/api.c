@@ -72,6 +72,77 @@ int fz_dev_malloc(void **p, size_t bytes)
     return 0;
 }
 
+static int device_usable(const void *p);
+
+aoclfftz_error_type aoclfftz_gpu_transpose(FFTZ_INT32 dtype, FFTZ_INT32 is_real, const FFTZ_VOID *in, FFTZ_VOID *out,
+                                           FFTZ_INT64 rows, FFTZ_INT64 cols, FFTZ_INT64 row_is, FFTZ_INT64 col_is,
+                                           FFTZ_INT64 row_os, FFTZ_INT64 col_os, FFTZ_VOID *stream)
+{
+    if (dtype != 0 && dtype != 1)
+    {
+        fz_set_error("transpose: dtype must be 0 (float) or 1 (double)");
+        return AOCLFFTZ_INVALID_INPUT;
+    }
+    if (is_real != 0 && is_real != 1)
+    {
+        fz_set_error("transpose: is_real must be 0 (complex) or 1 (real)");
+        return AOCLFFTZ_INVALID_INPUT;
+    }
+    if (rows < 1 || cols < 1 || row_is < 1 || col_is < 1 || row_os < 1 || col_os < 1)
+    {
+        fz_set_error("transpose: sizes and strides must be positive");
+        return AOCLFFTZ_INVALID_INPUT;
+    }
+    if (!in || !out)
+    {
+        fz_set_error("transpose: in and out cannot be NULL");
+        return AOCLFFTZ_INVALID_INPUT;
+    }
+    /* the largest element index on each side, and the element count, must
+     * fit 63 bits (checked without overflowing) */
+    if ((cols - 1) > INT64_MAX / col_is || (cols - 1) > INT64_MAX / col_os ||
+        (rows - 1) > (INT64_MAX - (cols - 1) * col_is) / row_is ||
+        (rows - 1) > (INT64_MAX - (cols - 1) * col_os) / row_os || rows > INT64_MAX / 16 / cols)
+    {
+        fz_set_error("transpose: the strides address beyond 2^63 elements");
+        return AOCLFFTZ_INVALID_INPUT;
+    }
+    if (!device_usable(in) || !device_usable(out))
+    {
+        fz_set_error("transpose: in and out must be device memory");
+        return AOCLFFTZ_INVALID_INPUT;
+    }
+    const int eb = (dtype == 0 ? 4 : 8) * (is_real ? 1 : 2);
+    cudaStream_t st = (cudaStream_t)stream;
+    int e;
+    if (in != out)
+        e = fftz_launch_transpose(in, out, rows, cols, row_is, col_is, row_os, col_os, eb, st);
+    else if (rows == cols && row_os == col_is && col_os == row_is)
+        e = fftz_launch_transpose_square_inplace(out, rows, row_is, col_is, eb, st);
+    else
+    {
+        /* any other in-place layout: copy the input to a dense temporary, then
+         * transpose from there */
+        void *tmp = NULL;
+        if (cudaMallocAsync(&tmp, (size_t)(rows * cols * eb), st) != cudaSuccess)
+        {
+            cudaGetLastError();
+            fz_set_error("transpose: temporary of %lld bytes could not be allocated", (long long)(rows * cols * eb));
+            return AOCLFFTZ_MEMORY_FAILURE;
+        }
+        e = fftz_launch_transpose(in, tmp, rows, cols, row_is, col_is, cols, 1, eb, st);
+        if (!e) e = fftz_launch_transpose(tmp, out, rows, cols, cols, 1, row_os, col_os, eb, st);
+        cudaFreeAsync(tmp, st);
+    }
+    if (e)
+    {
+        fz_set_error("transpose launch failed: %s", cudaGetErrorString((cudaError_t)e));
+        cudaGetLastError();
+        return AOCLFFTZ_EXECUTION_FAILURE;
+    }
+    return AOCLFFTZ_SUCCESS;
+}
+
 FFTZ_INT32 aoclfftz_gpu_inject_fault(FFTZ_INT32 kind, FFTZ_INT64 value)
 {
     if (value < 0) return -1;

@@ -188,6 +188,15 @@ typedef struct fftz_elem
 
 int fftz_launch_elem(const fftz_elem_t *e, void *stream);
 
+/* Standalone transpose (fft_transpose.cu): element (r, c) of a rows x cols
+ * array of elem_bytes-byte words from in[r * row_is + c * col_is] to
+ * out[r * row_os + c * col_os] (in != out); the square in-place form swaps
+ * (r, c) and (c, r) of data[r * row_s + c * col_s]. cudaError_t. */
+int fftz_launch_transpose(const void *in, void *out, int64_t rows, int64_t cols, int64_t row_is, int64_t col_is,
+                          int64_t row_os, int64_t col_os, int elem_bytes, void *stream);
+int fftz_launch_transpose_square_inplace(void *data, int64_t n, int64_t row_s, int64_t col_s, int elem_bytes,
+                                         void *stream);
+
 /* Largest in-SMEM transform length (complex elements) per dtype. */
 int fftz_max_smem_n(int dtype);
 

@@ -118,6 +118,9 @@ def bind_gpu(lib):
     lib.aoclfftz_gpu_last_error.restype = C.c_char_p
     lib.aoclfftz_gpu_inject_fault.argtypes = [C.c_int32, C.c_int64]
     lib.aoclfftz_gpu_inject_fault.restype = C.c_int32
+    lib.aoclfftz_gpu_transpose.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p] + [C.c_int64] * 6 + \
+        [C.c_void_p]
+    lib.aoclfftz_gpu_transpose.restype = C.c_int
     return lib
 
 

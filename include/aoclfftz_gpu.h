@@ -168,6 +168,26 @@ aoclfftz_error_type aoclfftz_gpu_execute_noalloc_c2c_f(const FFTZ_VOID *in, FFTZ
                                                        FFTZ_INT64 howmany, FFTZ_INT32 direction,
                                                        FFTZ_VOID *stream);
 
+/* Standalone transpose: the problem of the reference's transpose solver
+ * (core/solvers/transpose_solver.c:97-141), which the reference's public API
+ * does not reach (api/aoclfftz.h:97-99: transpose_mode must be 0, and
+ * aoclfftz_setup_* here rejects it the same way). Element (r, c) of a
+ * rows x cols array, r < rows, c < cols, is read at in[r * row_is + c * col_is]
+ * and written at out[r * row_os + c * col_os] (strides in elements, positive);
+ * a plain transpose of a dense row-major array is row_is = cols, col_is = 1,
+ * row_os = 1, col_os = rows. Elements are complex (is_real 0) or real
+ * (is_real 1), float (dtype 0) or double (dtype 1), moved bit-exactly. in and
+ * out are device memory that does not overlap unless in == out; in == out
+ * is allowed (a square in-place transpose
+ * swaps tiles in place, any other in-place layout goes through a temporary
+ * device buffer, stream-ordered). Enqueued on `stream` (NULL: the legacy
+ * default stream). Returns AOCLFFTZ_SUCCESS, AOCLFFTZ_INVALID_INPUT (with the
+ * reason in aoclfftz_gpu_last_error), AOCLFFTZ_MEMORY_FAILURE or
+ * AOCLFFTZ_EXECUTION_FAILURE. */
+aoclfftz_error_type aoclfftz_gpu_transpose(FFTZ_INT32 dtype, FFTZ_INT32 is_real, const FFTZ_VOID *in, FFTZ_VOID *out,
+                                           FFTZ_INT64 rows, FFTZ_INT64 cols, FFTZ_INT64 row_is, FFTZ_INT64 col_is,
+                                           FFTZ_INT64 row_os, FFTZ_INT64 col_os, FFTZ_VOID *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ typedef struct
 {
     fftz_ritem_t it;
     int depth;
+    int chain; /* passes of its plan from this one to the last */
     int64_t cost;
 } fz_item_sort;
 
@@ -34,6 +35,7 @@ static int item_cmp(const void *a, const void *b)
 {
     const fz_item_sort *x = (const fz_item_sort *)a, *y = (const fz_item_sort *)b;
     if (x->depth != y->depth) return x->depth < y->depth ? -1 : 1;
+    if (x->chain != y->chain) return x->chain > y->chain ? -1 : 1;
     if (x->cost != y->cost) return x->cost > y->cost ? -1 : 1;
     if (x->it.pass != y->it.pass) return x->it.pass < y->it.pass ? -1 : 1;
     return x->it.blk < y->it.blk ? -1 : (x->it.blk > y->it.blk);
@@ -292,6 +294,7 @@ static int add_group(rg_build *B, int64_t n, int64_t c, const int64_t *tin, cons
             it->it.signal = j + 1 < sub.npass;
             it->it.pad_ = 0;
             it->depth = j;
+            it->chain = sub.npass - j;
             it->cost = n;
         }
         prev_nblk = nblk;

@@ -279,6 +279,10 @@ static int add_group(rg_build *B, int64_t n, int64_t c, const int64_t *tin, cons
         B->indpos[B->npass][1] = (inddim[j] >= 0 && sp->dst == FZ_BUF_OUT) ? pout : -1;
         B->passes[B->npass] = k;
         const int64_t nblk = (k.ntf + k.tpc - 1) / k.tpc;
+        /* the tile's work, about tpc lines of n log2 n: longest first */
+        int64_t lg = 1;
+        while ((1LL << lg) < k.n) lg++;
+        const int64_t tile_work = (int64_t)k.tpc * k.n * lg;
         if (grow((void **)&B->items, &B->cap_item, B->nitem + nblk, sizeof(fz_item_sort), 4096))
         {
             rc = -1;
@@ -295,7 +299,7 @@ static int add_group(rg_build *B, int64_t n, int64_t c, const int64_t *tin, cons
             it->it.pad_ = 0;
             it->depth = j;
             it->chain = sub.npass - j;
-            it->cost = n;
+            it->cost = tile_work;
         }
         prev_nblk = nblk;
         B->npass++;
